@@ -1,0 +1,118 @@
+"""Generates the golden fixtures in tests/golden/ from the reference's own build.
+
+    python tests/golden/make_golden.py pre            # CPU, needs the reference sources
+    python tests/golden/make_golden.py ref OUTDIR     # on a B200, runs the reference's
+                                                      # FP64 CUDA solver (oracle/_ref)
+
+`pre` runs the reference's preprocessing (FAME_Preprocessing) through
+oracle/_ref/fame_ref_harness for every named workload and stores its integer and
+geometric outputs (grid, m1-m4, Omega, k path, Binout, ...) as <name>_pre.npz.
+
+`ref` runs the reference's FP64 solver on the small workloads and on the 96^3
+metric workload's first k-points, writing <name>_ref.json (frequencies, counters)
+and <name>_apply.npz (reference Qr/Qrs/QBQ/invAr applied to seeded vectors).
+The outputs are copied into tests/golden/ by hand after the run.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import ref_inputs as ri  # noqa: E402
+
+GOLDEN = os.path.dirname(os.path.abspath(__file__))
+
+PRE_NAMES = ["sc16", "sc32", "sc96", "fcc16", "fcc64", "bcc12", "bcc48", "hex12", "hex128"]
+
+
+def material_dict(name):
+    m = ri.WORKLOADS[name][0]()
+    nm = m["material_num"]
+    r12 = lambda v: [float(f"{float(x):.12f}") for x in v]  # as written to the file
+    return dict(
+        material_num=nm,
+        sphere_num=[sum(1 for s in m["spheres"] if s[0] == k) for k in range(nm)],
+        sphere_centers=r12([c for k in range(nm) for s in m["spheres"] if s[0] == k for c in s[1]]),
+        sphere_radius=r12([s[2] for k in range(nm) for s in m["spheres"] if s[0] == k]),
+        cylinder_num=[sum(1 for s in m["cylinders"] if s[0] == k) for k in range(nm)],
+        cylinder_top_centers=r12([c for k in range(nm) for s in m["cylinders"] if s[0] == k for c in s[1]]),
+        cylinder_bot_centers=r12([c for k in range(nm) for s in m["cylinders"] if s[0] == k for c in s[2]]),
+        cylinder_radius=r12([s[3] for k in range(nm) for s in m["cylinders"] if s[0] == k]),
+        lattice_type=m["lattice_type"], const=list(m["const"]))
+
+
+def do_pre():
+    for name in PRE_NAMES:
+        with tempfile.TemporaryDirectory() as d:
+            ri.make_workdir(name, d)
+            p = ri.run_pre(d, os.path.join(d, "pre.bin"))
+        binout = p.pop("Binout").astype(np.uint8)
+        np.savez_compressed(os.path.join(GOLDEN, f"{name}_pre.npz"),
+                            Binout_bits=np.packbits(binout), Binout_len=binout.size,
+                            material=json.dumps(material_dict(name)), **p)
+        print(name, p["grid_nums"], int(binout.sum()))
+
+
+# k-point subsets solved by the reference on the GPU: (workload, kidx or None=all, nwant)
+REF_RUNS = [
+    ("sc16", None),
+    ("fcc16", None),
+    ("bcc12", None),
+    ("hex12", None),
+    ("sc32", "0,1,3"),
+    ("sc96", "0,1"),
+]
+
+
+def do_ref(outdir):
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(1234)
+    for name, kidx in REF_RUNS:
+        with tempfile.TemporaryDirectory() as d:
+            ri.make_workdir(name, d)
+            out = os.path.join(outdir, f"{name}_ref.jsonl")
+            cmd = [ri.REF_HARNESS, "solve", d, out]
+            if kidx:
+                cmd += ["--kidx", kidx]
+            with open(os.path.join(outdir, f"{name}_ref.log"), "w") as log:
+                subprocess.run(cmd, check=True, stdout=log, stderr=subprocess.STDOUT)
+            if name.endswith("96") or name == "sc32":
+                continue
+            g = np.load(os.path.join(GOLDEN, f"{name}_pre.npz"))
+            N = int(np.prod(g["grid_nums"]))
+            x = rng.standard_normal(5 * N) + 1j * rng.standard_normal(5 * N)
+            inp = os.path.join(d, "in.bin")
+            x.astype("<c16").tofile(inp)
+            outb = os.path.join(d, "apply.bin")
+            with open(os.path.join(outdir, f"{name}_apply.log"), "w") as log:
+                subprocess.run([ri.REF_HARNESS, "apply", d, inp, outb], check=True,
+                               stdout=log, stderr=subprocess.STDOUT)
+            raw = np.fromfile(outb, "<f8")
+            nk = g["WaveVector"].size // 3
+            recs = {}
+            p = 0
+            for k in range(nk):
+                Nd = int(raw[p]); p += 1
+                for key, n in (("Qr", 3 * N), ("Qrs", 2 * Nd), ("QBQ", 2 * Nd), ("invAr", 2 * Nd)):
+                    v = raw[p:p + 2 * n].view("<c16")
+                    p += 2 * n
+                    recs[f"{key}_{k}"] = v.copy()
+                recs[f"Nd_{k}"] = np.array(Nd)
+            np.savez_compressed(os.path.join(outdir, f"{name}_apply.npz"), x=x, **recs)
+        print("done", name)
+
+
+if __name__ == "__main__":
+    if sys.argv[1] == "pre":
+        do_pre()
+    elif sys.argv[1] == "ref":
+        do_ref(sys.argv[2])
+    else:
+        raise SystemExit(__doc__)
