@@ -1,0 +1,97 @@
+// Shared device/host definitions for the FAME B200 band-structure library.
+//
+// Complex values are stored interleaved (re, im) as float2 / double2, the same
+// memory layout as cuDoubleComplex and the reference's `double _Complex` vectors,
+// so host buffers from the reference (FAME_Main/FAME_Main_Code.cu:53-54) can be
+// copied in and out unchanged.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fame {
+
+template <typename R> struct C2;
+template <> struct C2<float> { using T = float2; };
+template <> struct C2<double> { using T = double2; };
+template <typename R> using cplx = typename C2<R>::T;
+
+template <typename R> __host__ __device__ __forceinline__ cplx<R> mk(R a, R b) {
+  cplx<R> z;
+  z.x = a;
+  z.y = b;
+  return z;
+}
+template <typename T> __host__ __device__ __forceinline__ T cadd(T a, T b) {
+  T z;
+  z.x = a.x + b.x;
+  z.y = a.y + b.y;
+  return z;
+}
+template <typename T> __host__ __device__ __forceinline__ T csub(T a, T b) {
+  T z;
+  z.x = a.x - b.x;
+  z.y = a.y - b.y;
+  return z;
+}
+template <typename T> __host__ __device__ __forceinline__ T cmul(T a, T b) {
+  T z;
+  z.x = a.x * b.x - a.y * b.y;
+  z.y = a.x * b.y + a.y * b.x;
+  return z;
+}
+// conj(a) * b
+template <typename T> __host__ __device__ __forceinline__ T cmulc(T a, T b) {
+  T z;
+  z.x = a.x * b.x + a.y * b.y;
+  z.y = a.x * b.y - a.y * b.x;
+  return z;
+}
+template <typename T, typename S> __host__ __device__ __forceinline__ T cscale(T a, S s) {
+  T z;
+  z.x = a.x * s;
+  z.y = a.y * s;
+  return z;
+}
+template <typename T> __host__ __device__ __forceinline__ T cconj(T a) {
+  T z;
+  z.x = a.x;
+  z.y = -a.y;
+  return z;
+}
+template <typename T> __host__ __device__ __forceinline__ auto cabs2(T a) -> decltype(a.x) {
+  return a.x * a.x + a.y * a.y;
+}
+__host__ __device__ __forceinline__ float2 to_f(double2 a) {
+  return make_float2((float)a.x, (float)a.y);
+}
+__host__ __device__ __forceinline__ double2 to_d(float2 a) {
+  return make_double2((double)a.x, (double)a.y);
+}
+template <typename R> __device__ __forceinline__ cplx<R> cvt(double2 a);
+template <> __device__ __forceinline__ float2 cvt<float>(double2 a) { return to_f(a); }
+template <> __device__ __forceinline__ double2 cvt<double>(double2 a) { return a; }
+
+// e^{i*pi*x} evaluated with the CUDA math library's sincospi (argument in units of pi).
+__device__ __forceinline__ double2 expipi(double x) {
+  double s, c;
+  sincospi(x, &s, &c);
+  return make_double2(c, s);
+}
+__device__ __forceinline__ float2 expipi(float x) {
+  float s, c;
+  sincospif(x, &s, &c);
+  return make_float2(c, s);
+}
+
+// Status codes returned through the C ABI (include/fame_b200.h).
+enum Status : int {
+  kOk = 0,
+  kBadInput = 1,
+  kNoConvergence = 2,
+  kWatchdog = 3,
+  kCudaError = 4,
+  kNoDevice = 5,
+  kUnsupported = 6,
+};
+
+}  // namespace fame

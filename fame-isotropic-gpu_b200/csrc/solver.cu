@@ -1,0 +1,1125 @@
+// Host orchestration and the C ABI (include/fame_b200.h).
+//
+// One context = one device, one grid and lattice, one set of edge permittivities.
+// fame_solve_kpoints splits the k list into batches of `batch` k-points ("slots").
+// A batch runs the reference's whole per-k solve (FAME_Main/FAME_Fast_Algorithms_
+// Isotropic.cu:20-86: restarted Lanczos on A_r^{-1}, invAr by CG, Ritz vectors,
+// eigenvector restoration, Gamma patch) for all its slots in lockstep: every kernel
+// carries the slot in blockIdx.z and slots that finished skip their work.  The whole
+// batch is recorded once as a CUDA graph with WHILE nodes for the CG, refinement and
+// restart loops and replayed for every batch.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <utility>
+
+#include "../../include/fame_b200.h"
+#include "program.h"
+#include "solver_kernels.cuh"
+
+namespace fame {
+
+static thread_local std::string g_err;
+static void set_err(const std::string& s) { g_err = s; }
+
+// ------------------------------------------------------------------ FFT plans
+static bool factorize(int n, AxisPlan& p) {
+  p.n = n;
+  p.npass = 0;
+  int m = n;
+  const int order[] = {8, 4, 2, 5, 3, 7, 11, 13};
+  for (int r : order) {
+    while (m % r == 0) {
+      if (p.npass >= kMaxPasses) return false;
+      p.radix[p.npass++] = r;
+      m /= r;
+    }
+  }
+  for (int q = 17; m > 1 && q <= m; q++) {
+    while (m % q == 0) {
+      if (p.npass >= kMaxPasses) return false;
+      p.radix[p.npass++] = q;
+      m /= q;
+    }
+  }
+  if (n == 1) {
+    p.npass = 0;
+  }
+  return m == 1;
+}
+
+static void init_fft_constants() {
+  static bool done = false;
+  if (done) return;
+  auto fill = [](const void* sym_c, const void* sym_s, int r) {
+    std::vector<double> c(r), s(r);
+    for (int m = 0; m < r; m++) {
+      c[m] = cos(2.0 * M_PI * m / r);
+      s[m] = sin(2.0 * M_PI * m / r);
+    }
+    FAME_CK(cudaMemcpyToSymbol(sym_c, c.data(), r * sizeof(double)));
+    FAME_CK(cudaMemcpyToSymbol(sym_s, s.data(), r * sizeof(double)));
+  };
+  fill(c_cos5, c_sin5, 5);
+  fill(c_cos7, c_sin7, 7);
+  fill(c_cos11, c_sin11, 11);
+  fill(c_cos13, c_sin13, 13);
+  done = true;
+}
+
+// ------------------------------------------------------------------ device buffers
+template <typename T> struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void ensure(size_t count) {
+    if (count <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    FAME_CK(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace fame
+
+using namespace fame;
+
+struct fame_ctx {
+  int device = 0;
+  fame_lattice lat;
+  Geom g;
+  cudaStream_t stream = nullptr;
+  int plane_threads = 512;
+  bool have_eps = false;
+  // persistent data
+  DBuf<double2> tw64;
+  DBuf<float2> tw32;
+  DBuf<double> invB64, B64;
+  DBuf<float> invB32;
+  // per-batch workspace
+  int cap_slots = 0, cap_nstep = 0, cap_nwant = 0;
+  bool cap_mixed = false, cap_vec = false;
+  DBuf<Slot> slots;
+  DBuf<double2> tabs;
+  DBuf<CgState> cg;
+  DBuf<LzState> lz;
+  DBuf<double> partials, T0, T1, hcoef, theta, Z, G, stats;
+  DBuf<unsigned> counters, tri_ctr;
+  DBuf<int> map, prof, status, flags;
+  DBuf<double2> U, r64, x64, b64, p64, Ap64, T64, EV, AV, Tb, E;
+  DBuf<float2> r32, x32, p32, Ap32, T32;
+  int* hflag = nullptr;  // pinned
+  // recorded programs keyed by configuration
+  std::map<std::string, std::unique_ptr<Program>> progs;
+};
+
+namespace fame {
+
+static int vec_blocks(const fame_ctx* c, int nslots) {
+  const long n = 2L * c->g.N;
+  long b = (n + 2047) / 2048;
+  const long cap = std::max<long>(1, 1184 / std::max(1, nslots));
+  return (int)std::max<long>(1, std::min(b, cap));
+}
+
+template <typename R> static size_t plane_smem(const Geom& g) {
+  return sizeof(cplx<R>) * ((size_t)g.P + g.Lf + g.Lm);
+}
+template <typename R> static int pencil_tw() { return sizeof(R) == 8 ? 16 : 32; }
+template <typename R> static size_t pencil_smem(const Geom& g) {
+  return sizeof(cplx<R>) * ((size_t)g.Ls * pencil_tw<R>() + g.Ls);
+}
+
+template <typename K> static void allow_smem(K* k, size_t bytes) {
+  if (bytes > 48 * 1024) FAME_CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+struct Ops {
+  fame_ctx* c;
+  Program& P;
+  int nslots;
+
+  const Geom& g() const { return c->g; }
+
+  VecArgs va(Cond cond) const {
+    VecArgs v;
+    v.g = c->g;
+    v.slots = c->slots.p;
+    v.tabs = c->tabs.p;
+    v.vstride = 2L * c->g.N;
+    v.cg = c->cg.p;
+    v.partials = c->partials.p;
+    v.counters = c->counters.p;
+    v.cond = cond;
+    v.nslots = nslots;
+    return v;
+  }
+
+  template <typename R> const cplx<R>* tw() const;
+
+  // plane inverse stage
+  template <typename R, int IN, bool PR>
+  void plane_inv(const cplx<R>* in, cplx<R>* T, int nvec, long vstride, long fstride, int sigma,
+                 cplx<R>* p = nullptr, const cplx<R>* r = nullptr, double2* y64 = nullptr,
+                 const float2* x32 = nullptr) {
+    PlaneInArgs<R> a;
+    a.g = g();
+    a.slots = c->slots.p;
+    a.tabs = c->tabs.p;
+    a.tw = tw<R>();
+    a.vstride = vstride;
+    a.fstride = fstride;
+    a.vec_per_slot = nvec;
+    a.in = in;
+    a.p = p;
+    a.r = r;
+    a.cg = c->cg.p;
+    a.y64 = y64;
+    a.x32 = x32;
+    a.sigma = sigma;
+    a.T = T;
+    const size_t sm = plane_smem<R>(g());
+    dim3 grid(3 * g().Ls, nvec, nslots);
+    if (g().general) {
+      auto k = k_plane_inv<R, true, IN, PR>;
+      allow_smem(k, sm);
+      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+    } else {
+      auto k = k_plane_inv<R, false, IN, PR>;
+      allow_smem(k, sm);
+      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+    }
+  }
+
+  template <typename R, int MODE>
+  void pencil(cplx<R>* T, int nvec, long fstride, const R* invB, int gate, cplx<R>* out = nullptr,
+              const cplx<R>* in = nullptr) {
+    PencilArgs<R> a;
+    a.g = g();
+    a.slots = c->slots.p;
+    a.tabs = c->tabs.p;
+    a.tw = tw<R>();
+    a.fstride = fstride;
+    a.vec_per_slot = nvec;
+    a.T = T;
+    a.invB = invB;
+    a.out = out;
+    a.in = in;
+    a.cg = c->cg.p;
+    a.gate = gate;
+    a.TW = pencil_tw<R>();
+    const size_t sm = pencil_smem<R>(g());
+    const int nft = (g().Lf + a.TW - 1) / a.TW;
+    dim3 grid(g().Lm * nft, 3 * nvec, nslots);
+    if (g().general) {
+      auto k = k_pencil<R, true, MODE>;
+      allow_smem(k, sm);
+      P.launch(k, grid, dim3(256), sm, a);
+    } else {
+      auto k = k_pencil<R, false, MODE>;
+      allow_smem(k, sm);
+      P.launch(k, grid, dim3(256), sm, a);
+    }
+  }
+
+  template <typename R, int EPI, bool PR>
+  void plane_fwd(const cplx<R>* T, cplx<R>* out, int nvec, long vstride, long fstride,
+                 const cplx<R>* p = nullptr, const cplx<R>* b = nullptr, Cond cond = Cond{0, nullptr},
+                 double tol2 = 0) {
+    PlaneOutArgs<R> a;
+    a.g = g();
+    a.slots = c->slots.p;
+    a.tabs = c->tabs.p;
+    a.tw = tw<R>();
+    a.vstride = vstride;
+    a.fstride = fstride;
+    a.vec_per_slot = nvec;
+    a.T = T;
+    a.out = out;
+    a.p = p;
+    a.b = b;
+    a.cg = c->cg.p;
+    a.partials = c->partials.p;
+    a.counters = c->counters.p;
+    a.cond = cond;
+    a.nslots = nslots;
+    a.tol2 = tol2;
+    const size_t sm = plane_smem<R>(g());
+    dim3 grid(3 * g().Ls, nvec, nslots);
+    if (g().general) {
+      auto k = k_plane_fwd<R, true, EPI, PR>;
+      allow_smem(k, sm);
+      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+    } else {
+      auto k = k_plane_fwd<R, false, EPI, PR>;
+      allow_smem(k, sm);
+      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+    }
+  }
+};
+template <> const double2* Ops::tw<double>() const { return c->tw64.p; }
+template <> const float2* Ops::tw<float>() const { return c->tw32.p; }
+
+// ------------------------------------------------------------------ geometry
+static int setup_geom(fame_ctx* c) {
+  const fame_lattice& L = c->lat;
+  Geom& g = c->g;
+  memset(&g, 0, sizeof(g));
+  g.Nx = L.grid[0];
+  g.Ny = L.grid[1];
+  g.Nz = L.grid[2];
+  if (g.Nx < 2 || g.Ny < 2 || g.Nz < 2) {
+    set_err("grid dimensions must be >= 2");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const long N = (long)g.Nx * g.Ny * g.Nz;
+  if (N > (1L << 28)) {
+    set_err("grid too large");
+    return FAME_ERR_BAD_INPUT;
+  }
+  g.N = (int)N;
+  g.general = L.simple ? 0 : 1;
+  g.hx = L.mesh_len[0];
+  g.hy = L.mesh_len[1];
+  g.hz = L.mesh_len[2];
+  if (!g.general) {
+    g.Ls = g.Nz;
+    g.Lm = g.Ny;
+    g.Lf = g.Nx;
+  } else {
+    g.Ls = g.Nx;
+    g.Lm = g.Ny;
+    g.Lf = g.Nz;
+  }
+  g.P = g.Lm * g.Lf;
+  if (!factorize(g.Lf, g.pf) || !factorize(g.Lm, g.pm) || !factorize(g.Ls, g.ps)) {
+    set_err("axis length needs more than 10 FFT passes");
+    return FAME_ERR_UNSUPPORTED;
+  }
+  // the whole plane must fit one CTA's shared memory (FP64 copy)
+  c->plane_threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
+  if (plane_smem<double>(g) > 227 * 1024) {
+    set_err("plane " + std::to_string(g.Lm) + "x" + std::to_string(g.Lf) + " exceeds one CTA");
+    return FAME_ERR_UNSUPPORTED;
+  }
+  // table offsets
+  int o = 0;
+  if (!g.general) {
+    g.oLx = o; o += g.Nx;
+    g.oLy = o; o += g.Ny;
+    g.oLz = o; o += g.Nz;
+    g.oDx = o; o += g.Nx;
+    g.oDy = o; o += g.Ny;
+    g.oDz = o; o += g.Nz;
+  } else {
+    g.oLx = o; o += g.Nx;
+    g.oLy = o; o += g.Nx * g.Ny;
+    g.oExy = o; o += g.Nx * g.Ny;
+    g.oWz = o; o += g.Nz;
+    g.oDky = o; o += g.Nx * g.Ny;
+    g.oPhi = o; o += g.Nx * g.Ny;
+    g.oDkx = o; o += g.Nx;
+  }
+  g.tab_stride = (o + 7) / 8 * 8;
+  // twiddles e^{-2 pi i m / n} for the fast, mid and slow axes
+  std::vector<double2> tw;
+  auto add = [&](int n) {
+    const int off = (int)tw.size();
+    for (int m = 0; m < n; m++) tw.push_back(make_double2(cos(2.0 * M_PI * m / n), -sin(2.0 * M_PI * m / n)));
+    return off;
+  };
+  g.twf = add(g.Lf);
+  g.twm = add(g.Lm);
+  g.tws = add(g.Ls);
+  std::vector<float2> tw32(tw.size());
+  for (size_t i = 0; i < tw.size(); i++) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+  c->tw64.ensure(tw.size());
+  c->tw32.ensure(tw.size());
+  FAME_CK(cudaMemcpy(c->tw64.p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  FAME_CK(cudaMemcpy(c->tw32.p, tw32.data(), tw32.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  return FAME_OK;
+}
+
+// theta_x, theta_y(xy), theta_z(xyz) (FAME_Main/FAME_Matrix_Lambdas.cu:43-70)
+static void thetas(const fame_lattice& L, const double* k, double th[3]) {
+  const double* a = L.lattice_vec_a;
+  auto dot = [&](const double* v) { return k[0] * v[0] + k[1] * v[1] + k[2] * v[2]; };
+  th[0] = dot(a);
+  if (L.simple) {
+    th[1] = dot(a + 3);
+    th[2] = dot(a + 6);
+    return;
+  }
+  double c1 = 0.0;
+  if (a[3] > 0)
+    c1 = -(double)L.m[0] / (double)L.grid[0];
+  else if (a[3] < 0)
+    c1 = 1. - (double)L.m[0] / (double)L.grid[0];
+  const double c2 = (double)L.m[2] / (double)L.grid[1];
+  const double c3 = (double)L.m[1] / (double)L.grid[0];
+  double a2h[3], a3h[3];
+  for (int i = 0; i < 3; i++) a2h[i] = c1 * a[i] + a[3 + i];
+  for (int i = 0; i < 3; i++) a3h[i] = a[6 + i] - c2 * a2h[i] - c3 * a[i] + L.t1[i];
+  th[1] = dot(a2h);
+  th[2] = dot(a3h);
+}
+
+static int reduced_size(const fame_lattice& L, const double* k) {
+  const int N = L.grid[0] * L.grid[1] * L.grid[2];
+  const double nrm = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+  // Gamma point: Nd = N - 1 (…Lambdas.cu:157 Simple, threshold 1e-4; :406 General, 1e-3)
+  return nrm < (L.simple ? 1e-4 : 1e-3) ? N - 1 : N;
+}
+
+static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool mixed, bool vec) {
+  if (nslots <= c->cap_slots && nstep <= c->cap_nstep && nwant <= c->cap_nwant &&
+      (!mixed || c->cap_mixed) && (!vec || c->cap_vec))
+    return;
+  const Geom& g = c->g;
+  const size_t N = g.N, M = 2 * N;
+  nslots = std::max(nslots, c->cap_slots);
+  nstep = std::max(nstep, c->cap_nstep);
+  nwant = std::max(nwant, c->cap_nwant);
+  mixed = mixed || c->cap_mixed;
+  vec = vec || c->cap_vec;
+  c->progs.clear();
+  c->slots.ensure(nslots);
+  c->tabs.ensure((size_t)nslots * g.tab_stride);
+  c->cg.ensure(nslots);
+  c->lz.ensure(nslots);
+  const size_t lzblk = (M + kLzRows - 1) / kLzRows;
+  const size_t part = std::max({lzblk * (2 * 64 + 1), (size_t)3 * g.Ls * 2 * 16, (size_t)1184 * 4});
+  c->partials.ensure((size_t)nslots * part);
+  c->counters.ensure(nslots + 1);
+  FAME_CK(cudaMemset(c->counters.p, 0, (nslots + 1) * sizeof(unsigned)));
+  c->tri_ctr.ensure(1);
+  FAME_CK(cudaMemset(c->tri_ctr.p, 0, sizeof(unsigned)));
+  c->T0.ensure((size_t)nslots * nstep);
+  c->T1.ensure((size_t)nslots * nstep);
+  c->hcoef.ensure((size_t)nslots * 2 * (nstep + 2));
+  c->theta.ensure((size_t)nslots * nstep);
+  c->Z.ensure((size_t)nslots * nstep * nstep);
+  c->G.ensure((size_t)nslots * (nstep + 1) * (nwant + 1));
+  c->stats.ensure((size_t)nslots * nwant * 8);
+  c->map.ensure((size_t)nslots * (nstep + 1) + (size_t)nslots * (nwant + 1));
+  c->prof.ensure((size_t)nslots * 2);
+  c->status.ensure(nslots);
+  c->flags.ensure(64);
+  const int nphys = nstep + 1 + nwant + 1;
+  c->U.ensure((size_t)nslots * nphys * M);
+  c->r64.ensure((size_t)nslots * M);
+  c->x64.ensure((size_t)nslots * M);
+  c->T64.ensure((size_t)nslots * 3 * N);
+  c->EV.ensure((size_t)nslots * nwant * M);
+  c->AV.ensure((size_t)nslots * nwant * M);
+  c->Tb.ensure((size_t)nslots * nwant * 3 * N);
+  if (mixed) {
+    c->b64.ensure((size_t)nslots * M);
+    c->r32.ensure((size_t)nslots * M);
+    c->x32.ensure((size_t)nslots * M);
+    c->p32.ensure((size_t)nslots * M);
+    c->Ap32.ensure((size_t)nslots * M);
+    c->T32.ensure((size_t)nslots * 3 * N);
+  } else {
+    c->p64.ensure((size_t)nslots * M);
+    c->Ap64.ensure((size_t)nslots * M);
+  }
+  if (mixed && !c->p64.p) {
+    c->p64.ensure((size_t)nslots * M);
+    c->Ap64.ensure((size_t)nslots * M);
+  }
+  if (vec) c->E.ensure((size_t)nslots * nwant * 3 * N);
+  c->cap_slots = nslots;
+  c->cap_nstep = nstep;
+  c->cap_nwant = nwant;
+  c->cap_mixed = mixed;
+  c->cap_vec = vec;
+}
+
+// ------------------------------------------------------------------ statistics kernels
+// Per (slot, band): y = Ritz vector, v = QBQ(Sigma y).  Reduces
+// ||Sigma (Sigma v - lambda y)||^2, ||Sigma y||^2, Re<Sigma y, v>, ||y||^2.
+__global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* EV, const double2* AV,
+                                                    long vstride, int nwant, const double* theta,
+                                                    int nstep, double* stats) {
+  const int band = blockIdx.y, slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  if (!sl.active) return;
+  const double lam = 1.0 / theta[slot * nstep + band];
+  const double2* tab = va.tabs + (size_t)slot * va.g.tab_stride;
+  const long base = (long)(slot * nwant + band) * vstride;
+  const int n = 2 * sl.Nd;
+  double acc[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double s = lq_sqrt_at(va.g, tab, full_index(i, sl.Nd, sl.off));
+    const double2 y = EV[base + i], v = AV[base + i];
+    const double rx = s * (s * v.x - lam * y.x), ry = s * (s * v.y - lam * y.y);
+    acc[0] += rx * rx + ry * ry;
+    acc[1] += s * s * (y.x * y.x + y.y * y.y);
+    acc[2] += s * (y.x * v.x + y.y * v.y);
+    acc[3] += y.x * y.x + y.y * y.y;
+  }
+  __shared__ double sred[4 * 32];
+  block_reduce<4>(acc, sred);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 4; q++) stats[((size_t)slot * nwant + band) * 4 + q] = acc[q];
+}
+
+// ||E||^2 per (slot, band) and the reference's scaling E *= ||E||
+// (FAME_Fast_Algorithms_Isotropic.cu:119-121).
+__global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, double2* E, long fstride,
+                                                          int nwant, long n3) {
+  const int band = blockIdx.x, slot = blockIdx.y;
+  if (!slots[slot].active) return;
+  double2* e = E + (long)(slot * nwant + band) * fstride;
+  double acc[1] = {0.0};
+  for (long i = threadIdx.x; i < n3; i += blockDim.x) acc[0] += cabs2(e[i]);
+  __shared__ double sred[32];
+  block_reduce<1>(acc, sred);
+  __shared__ double nrm;
+  if (threadIdx.x == 0) nrm = sqrt(acc[0]);
+  __syncthreads();
+  const double s = nrm;
+  for (long i = threadIdx.x; i < n3; i += blockDim.x) e[i] = cscale(e[i], s);
+}
+
+// ------------------------------------------------------------------ adjoint
+// Hellmann-Feynman for C^H C E = w^2 B E with diagonal B: d(w^2)/dB_e =
+// -w^2 |E_e|^2 / (E^H B E), so dw/dB_e = -(w/2) |E_e|^2 / (E^H B E).  With one
+// permittivity per voxel (B_x = B_y = B_z = eps) the voxel gradient sums its three
+// edges.  Bands with w = 0 (Gamma patch) get zero gradient.
+__global__ void __launch_bounds__(1024) k_adj_den(const double2* E, const double* B, long n3, double* den) {
+  const int band = blockIdx.x;
+  const double2* e = E + (long)band * n3;
+  double acc[1] = {0.0};
+  for (long i = threadIdx.x; i < n3; i += blockDim.x) acc[0] += B[i] * cabs2(e[i]);
+  __shared__ double sred[32];
+  block_reduce<1>(acc, sred);
+  if (threadIdx.x == 0) den[band] = acc[0];
+}
+
+__global__ void __launch_bounds__(256) k_adj_grad(const double2* E, const double* w, const double* den, long N,
+                                                  double* grad) {
+  const int band = blockIdx.y;
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const double2* e = E + (long)band * 3 * N;
+  const double s = cabs2(e[v]) + cabs2(e[N + v]) + cabs2(e[2 * N + v]);
+  grad[(long)band * N + v] = w[band] > 0 ? -0.5 * w[band] * s / den[band] : 0.0;
+}
+
+// ------------------------------------------------------------------ recording
+struct SolveCfg {
+  int nslots, nstep, nwant, es_maxit, ls_maxit, mixed, vec, inner_maxit;
+  double es_tol, ls_tol, inner_tol;
+};
+
+static std::string cfg_key(const SolveCfg& s, bool graph) {
+  char b[256];
+  snprintf(b, sizeof b, "%d/%d/%d/%d/%d/%d/%d/%d/%.17g/%.17g/%.17g/%d", s.nslots, s.nstep, s.nwant, s.es_maxit,
+           s.ls_maxit, s.mixed, s.vec, s.inner_maxit, s.es_tol, s.ls_tol, s.inner_tol, (int)graph);
+  return b;
+}
+
+// invAr (FAME_Main/FAME_Matrix_Vector_Production_Isotropic_invAr.cu:8-48) for the
+// Lanczos vector u_j of every live slot, leaving w in U[:, j+1]; then one Lanczos step.
+static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base) {
+  fame_ctx* c = o.c;
+  Program& P = o.P;
+  const Geom& g = c->g;
+  const int nvb = vec_blocks(c, s.nslots);
+  const long M = 2L * g.N;
+  const long F = 3L * g.N;
+  const double tol2 = s.ls_tol * s.ls_tol;
+  if (!s.mixed) {
+    Cond cc = P.make_cond(flag_base + 0);
+    P.launch(k_invar_pro<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), L, j, c->r64.p, c->x64.p,
+             (double2*)nullptr, tol2, s.ls_maxit);
+    P.while_loop(cc, [&] {
+      o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p);
+      o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 1);
+      o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
+      P.launch(k_cg_update<double>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
+               (const double2*)c->p64.p, (const double2*)c->Ap64.p);
+    });
+    P.launch(k_invar_epi<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j,
+             (const double2*)c->x64.p);
+  } else {
+    Cond outer = P.make_cond(flag_base + 1);
+    Cond inner = P.make_cond(flag_base + 2);
+    P.launch(k_invar_pro<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(outer), L, j, c->r64.p, c->x64.p,
+             c->b64.p, tol2, s.ls_maxit);
+    P.while_loop(outer, [&] {
+      P.launch(k_cg32_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), (const double2*)c->r64.p,
+               c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit);
+      P.while_loop(inner, [&] {
+        o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p);
+        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 1);
+        o.plane_fwd<float, EPI_CG, false>(c->T32.p, c->Ap32.p, 1, M, F, c->p32.p);
+        P.launch(k_cg_update<float>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), c->x32.p, c->r32.p,
+                 (const float2*)c->p32.p, (const float2*)c->Ap32.p);
+      });
+      o.plane_inv<double, IN_REFINE, false>(nullptr, c->T64.p, 1, M, F, 0, nullptr, nullptr, c->x64.p,
+                                            c->x32.p);
+      o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 2);
+      o.plane_fwd<double, EPI_RESID, false>(c->T64.p, c->r64.p, 1, M, F, nullptr, c->b64.p, outer, tol2);
+    });
+    P.launch(k_invar_epi<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j,
+             (const double2*)c->x64.p);
+  }
+  const int ndots = (int)((M + kLzRows - 1) / kLzRows);
+  P.launch(k_lz_dots, dim3(ndots, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j);
+  P.launch(k_lz_update, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j);
+}
+
+static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
+  Ops o{c, P, s.nslots};
+  const Geom& g = c->g;
+  const long M = 2L * g.N;
+  const long F = 3L * g.N;
+  const int nvb = vec_blocks(c, s.nslots);
+  const int nphys = s.nstep + 1 + s.nwant + 1;
+  LzArgs L;
+  L.U = c->U.p;
+  L.ustride = M;
+  L.nphys = nphys;
+  L.map = c->map.p;
+  L.nstep = s.nstep;
+  L.nwant = s.nwant;
+  L.T0 = c->T0.p;
+  L.T1 = c->T1.p;
+  L.h = c->hcoef.p;
+  L.lz = c->lz.p;
+  L.prof = c->prof.p;
+  int* flags = c->flags.p;
+  const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
+  P.launch(k_tables, dim3((tmax + 255) / 256, s.nslots), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
+           (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
+  P.launch(k_lz_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}), L);
+  for (int j = 0; j < s.nstep; j++) emit_step(o, s, L, j, flags);
+  Cond restart = P.make_cond(flags + 4);
+  TriArgs ta;
+  ta.L = L;
+  ta.slots = c->slots.p;
+  ta.theta = c->theta.p;
+  ta.Z = c->Z.p;
+  ta.G = c->G.p;
+  ta.tol = s.es_tol;
+  ta.maxit = s.es_maxit;
+  ta.cond = restart;
+  ta.nslots = s.nslots;
+  ta.status = c->status.p;
+  ta.ctr = c->tri_ctr.p;
+  const size_t tsm = tridiag_smem(s.nstep);
+  allow_smem(k_tridiag, tsm);
+  P.launch(k_tridiag, dim3(s.nslots), dim3(32), tsm, ta);
+  P.while_loop(restart, [&] {
+    for (int c0 = 0; c0 <= s.nwant; c0 += 8)
+      P.launch(k_ugemm<8>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}), L,
+               (const double*)c->G.p, s.nstep + 1, s.nstep + 1, s.nwant + 1, 0, (double2*)nullptr, c0);
+    P.launch(k_remap, dim3(s.nslots), dim3(32), 0, L, (const Slot*)c->slots.p, s.nslots);
+    for (int j = s.nwant; j < s.nstep; j++) emit_step(o, s, L, j, flags);
+    P.launch(k_tridiag, dim3(s.nslots), dim3(32), tsm, ta);
+  });
+  // Ritz vectors ev = U(:, 0:nstep) z(:, 0:nwant)   (Lanczos_Isotropic.cu:93)
+  for (int c0 = 0; c0 < s.nwant; c0 += 8)
+    P.launch(k_ugemm<8>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}), L, (const double*)c->Z.p,
+             s.nstep, s.nstep, s.nwant, 1, c->EV.p, c0);
+  // FP64 residual and Rayleigh quotient per band: v = QBQ(Sigma y)
+  o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
+  o.pencil<double, PEN_QBQ>(c->Tb.p, s.nwant, F, c->invB64.p, 0);
+  o.plane_fwd<double, EPI_OUT, false>(c->Tb.p, c->AV.p, s.nwant, M, F);
+  P.launch(k_band_stats, dim3(1, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}),
+           (const double2*)c->EV.p, (const double2*)c->AV.p, M, s.nwant, (const double*)c->theta.p, s.nstep,
+           c->stats.p);
+  if (s.vec) {
+    // E = B^{-1} Q_r (Sigma ev), scaled by its norm (FAME_Fast_Algorithms_Isotropic.cu:107-122)
+    o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
+    o.pencil<double, PEN_QR_OUT>(c->Tb.p, s.nwant, F, c->invB64.p, 0, c->E.p);
+    P.launch(k_band_norm_scale, dim3(s.nwant, s.nslots), dim3(1024), 0, (const Slot*)c->slots.p, c->E.p, F,
+             s.nwant, F);
+  }
+}
+
+static int choose_batch(const fame_ctx* c, int nk, const fame_solver_params* p) {
+  if (p->batch > 0) return std::min(p->batch, nk);
+  // keep one batch's CG working set (about 88 N bytes in FP32) inside the 126 MB L2
+  const double ws = 100.0 * c->g.N;
+  int b = (int)std::max(1.0, floor(90e6 / ws));
+  return std::max(1, std::min({b, nk, 32}));
+}
+
+}  // namespace fame
+
+// ================================================================== C ABI
+extern "C" {
+
+const char* fame_last_error(void) { return g_err.c_str(); }
+const char* fame_version(void) { return "fame-b200 0.1 (sm_100a)"; }
+
+int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out) {
+  if (!lat || !out) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_err("no CUDA device");
+    return FAME_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_err("device index out of range");
+    return FAME_ERR_BAD_INPUT;
+  }
+  fame_ctx* c = new fame_ctx();
+  try {
+    c->device = device;
+    c->lat = *lat;
+    FAME_CK(cudaSetDevice(device));
+    init_fft_constants();
+    int rc = setup_geom(c);
+    if (rc) {
+      delete c;
+      return rc;
+    }
+    FAME_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    FAME_CK(cudaMallocHost(&c->hflag, sizeof(int)));
+    c->invB64.ensure(3L * c->g.N);
+    c->B64.ensure(3L * c->g.N);
+    c->invB32.ensure(3L * c->g.N);
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    delete c;
+    return FAME_ERR_CUDA;
+  }
+  *out = c;
+  return FAME_OK;
+}
+
+void fame_ctx_destroy(fame_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->progs.clear();
+  for (auto* b : {&c->tw64, &c->tabs, &c->U, &c->r64, &c->x64, &c->b64, &c->p64, &c->Ap64, &c->T64, &c->EV,
+                  &c->AV, &c->Tb, &c->E})
+    b->release();
+  for (auto* b : {&c->r32, &c->x32, &c->p32, &c->Ap32, &c->T32, &c->tw32}) b->release();
+  for (auto* b : {&c->invB64, &c->B64, &c->partials, &c->T0, &c->T1, &c->hcoef, &c->theta, &c->Z, &c->G,
+                  &c->stats})
+    b->release();
+  c->invB32.release();
+  c->slots.release();
+  c->cg.release();
+  c->lz.release();
+  c->counters.release();
+  c->tri_ctr.release();
+  c->map.release();
+  c->prof.release();
+  c->status.release();
+  c->flags.release();
+  if (c->hflag) cudaFreeHost(c->hflag);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int fame_ctx_sizes(const fame_ctx* c, long long* N_out) {
+  if (!c || !N_out) return FAME_ERR_BAD_INPUT;
+  *N_out = c->g.N;
+  return FAME_OK;
+}
+
+int fame_set_eps(fame_ctx* c, const double* B) {
+  if (!c || !B) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const long n3 = 3L * c->g.N;
+  std::vector<double> ib(n3);
+  std::vector<float> ib32(n3);
+  for (long i = 0; i < n3; i++) {
+    if (!(B[i] > 0.0) || !isfinite(B[i])) {
+      set_err("permittivity must be finite and positive (edge " + std::to_string(i) + ")");
+      return FAME_ERR_BAD_INPUT;
+    }
+    ib[i] = 1.0 / B[i];
+    ib32[i] = (float)ib[i];
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    FAME_CK(cudaMemcpy(c->B64.p, B, n3 * sizeof(double), cudaMemcpyHostToDevice));
+    FAME_CK(cudaMemcpy(c->invB64.p, ib.data(), n3 * sizeof(double), cudaMemcpyHostToDevice));
+    FAME_CK(cudaMemcpy(c->invB32.p, ib32.data(), n3 * sizeof(float), cudaMemcpyHostToDevice));
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  c->have_eps = true;
+  return FAME_OK;
+}
+
+int fame_set_material(fame_ctx* c, const int* binout, int material_num, const double* eps_in, double eps_out) {
+  if (!c || !binout || (material_num > 0 && !eps_in)) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const long N = c->g.N;
+  std::vector<double> B(3 * N, eps_out);
+  for (int comp = 0; comp < 3; comp++)
+    for (long i = 0; i < N; i++)
+      for (int j = 0; j < material_num; j++)
+        if (binout[i + j * N + (long)comp * material_num * N] == 1) B[comp * N + i] = eps_in[j];
+  return fame_set_eps(c, B.data());
+}
+
+int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solver_params* prm,
+                       double* freq_out, double* relres_out, double* relerr_out, double* evec_out,
+                       fame_kcounters* counters) {
+  if (!c || !k_xyz || !prm || !freq_out || nk <= 0) {
+    set_err("null or empty argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (!c->have_eps) {
+    set_err("permittivity not set (fame_set_eps / fame_set_material)");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const fame_solver_params& p = *prm;
+  if (p.nwant < 1 || p.nstep <= p.nwant || p.nstep > kMaxStep || p.es_maxit < 0 || p.ls_maxit < 1 ||
+      !(p.es_tol > 0) || !(p.ls_tol > 0) || (p.precision != FAME_FP64 && p.precision != FAME_MIXED)) {
+    set_err("invalid solver parameters (need 1 <= nwant < nstep <= 64, positive tolerances)");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (p.want_vectors && !evec_out) {
+    set_err("want_vectors set but evec_out is NULL");
+    return FAME_ERR_BAD_INPUT;
+  }
+  int rc_all = FAME_OK;
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    SolveCfg s;
+    s.nslots = choose_batch(c, nk, &p);
+    s.nstep = p.nstep;
+    s.nwant = p.nwant;
+    s.es_maxit = p.es_maxit;
+    s.ls_maxit = p.ls_maxit;
+    s.mixed = p.precision == FAME_MIXED;
+    s.vec = p.want_vectors ? 1 : 0;
+    s.es_tol = p.es_tol;
+    s.ls_tol = p.ls_tol;
+    s.inner_tol = p.inner_tol > 0 ? p.inner_tol : 1e-5;
+    s.inner_maxit = p.inner_maxit > 0 ? p.inner_maxit : 200;
+    const bool graph = p.use_graph != 0;
+    ensure_workspace(c, s.nslots, s.nstep, s.nwant, s.mixed, s.vec);
+    const std::string key = cfg_key(s, graph);
+    auto it = c->progs.find(key);
+    Program* P;
+    if (graph) {
+      if (it == c->progs.end()) {
+        auto prog = std::make_unique<Program>(c->stream, true, c->hflag, 0);
+        record_solve(c, *prog, s);
+        prog->instantiate();
+        P = prog.get();
+        c->progs[key] = std::move(prog);
+      } else {
+        P = it->second.get();
+      }
+    }
+    const long N = c->g.N;
+    std::vector<Slot> hs(s.nslots);
+    std::vector<double> theta((size_t)s.nslots * s.nstep), stats((size_t)s.nslots * s.nwant * 4);
+    std::vector<LzState> lz(s.nslots);
+    std::vector<int> prof(2 * s.nslots), status(s.nslots);
+    for (int b0 = 0; b0 < nk; b0 += s.nslots) {
+      const int nb = std::min(s.nslots, nk - b0);
+      for (int q = 0; q < s.nslots; q++) {
+        Slot& sl = hs[q];
+        memset(&sl, 0, sizeof(sl));
+        if (q < nb) {
+          const double* k = k_xyz + 3L * (b0 + q);
+          thetas(c->lat, k, sl.th);
+          sl.Nd = reduced_size(c->lat, k);
+          sl.off = (int)N - sl.Nd;
+          sl.active = 1;
+        } else {
+          sl.Nd = (int)N;
+          sl.active = 0;
+        }
+      }
+      FAME_CK(cudaMemcpyAsync(c->slots.p, hs.data(), s.nslots * sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
+      FAME_CK(cudaMemsetAsync(c->status.p, 0, s.nslots * sizeof(int), c->stream));
+      if (graph) {
+        P->run();
+      } else {
+        Program hp(c->stream, false, c->hflag, 100000);
+        record_solve(c, hp, s);
+      }
+      FAME_CK(cudaMemcpyAsync(theta.data(), c->theta.p, theta.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+      FAME_CK(cudaMemcpyAsync(stats.data(), c->stats.p, stats.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+      FAME_CK(cudaMemcpyAsync(lz.data(), c->lz.p, lz.size() * sizeof(LzState), cudaMemcpyDeviceToHost, c->stream));
+      FAME_CK(cudaMemcpyAsync(prof.data(), c->prof.p, prof.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      FAME_CK(cudaMemcpyAsync(status.data(), c->status.p, status.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                              c->stream));
+      FAME_CK(cudaStreamSynchronize(c->stream));
+      for (int q = 0; q < nb; q++) {
+        const int kk = b0 + q;
+        const bool gamma = hs[q].Nd == N - 1;
+        std::vector<double> f(s.nwant), rr(s.nwant), re(s.nwant);
+        for (int i = 0; i < s.nwant; i++) {
+          const double th = theta[(size_t)q * s.nstep + i];
+          f[i] = sqrt(1.0 / th);
+          const double* st = &stats[((size_t)q * s.nwant + i) * 4];
+          const double lam = 1.0 / th;
+          rr[i] = sqrt(st[0]) / (lam * sqrt(st[1]));
+          const double rho = st[2] / st[3];
+          re[i] = fabs(lam - rho) / rho;
+        }
+        // Gamma patch: bands shift up by two, w0 = w1 = 0 (FAME_Fast_Algorithms_Isotropic.cu:61-79)
+        std::vector<double> fo(f), ro(rr), eo(re);
+        if (gamma) {
+          for (int i = s.nwant - 1; i >= 2; i--) {
+            fo[i] = f[i - 2];
+            ro[i] = rr[i - 2];
+            eo[i] = re[i - 2];
+          }
+          fo[0] = fo[1] = 0.0;
+          ro[0] = ro[1] = 0.0;
+          eo[0] = eo[1] = 0.0;
+        }
+        for (int i = 0; i < s.nwant; i++) {
+          freq_out[(size_t)kk * s.nwant + i] = fo[i];
+          if (relres_out) relres_out[(size_t)kk * s.nwant + i] = ro[i];
+          if (relerr_out) relerr_out[(size_t)kk * s.nwant + i] = eo[i];
+        }
+        if (counters) {
+          fame_kcounters& kc = counters[kk];
+          kc.ls_iter = prof[2 * q];
+          kc.es_iter = prof[2 * q + 1];
+          kc.restarts = lz[q].restarts;
+          kc.status = status[q] == 0 ? FAME_OK : FAME_ERR_NO_CONVERGENCE;
+          kc.Nd = hs[q].Nd;
+          kc.pad = 0;
+        }
+        if (status[q] != 0) rc_all = FAME_ERR_NO_CONVERGENCE;
+        if (s.vec) {
+          const size_t n3 = 3 * (size_t)N;
+          double2* dst = reinterpret_cast<double2*>(evec_out) + (size_t)kk * s.nwant * n3;
+          const double2* src = c->E.p + (size_t)q * s.nwant * n3;
+          if (!gamma) {
+            FAME_CK(cudaMemcpy(dst, src, s.nwant * n3 * sizeof(double2), cudaMemcpyDeviceToHost));
+          } else {
+            if (s.nwant > 2)
+              FAME_CK(cudaMemcpy(dst + 2 * n3, src, (s.nwant - 2) * n3 * sizeof(double2), cudaMemcpyDeviceToHost));
+            const double v = 1.0 / sqrt(3.0 * N);
+            for (size_t i = 0; i < 2 * n3; i++) dst[i] = make_double2(v, 0.0);
+          }
+        }
+      }
+    }
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  } catch (const std::exception& e) {
+    set_err(e.what());
+    return FAME_ERR_WATCHDOG;
+  }
+  if (rc_all) set_err("Lanczos did not converge within es_maxit restarts for some k-point");
+  return rc_all;
+}
+
+int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, int precision,
+               const fame_solver_params* prm, int* Nd_out) {
+  if (!c || !k || !in || !out) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (op < FAME_OP_QR || op > FAME_OP_INVAR || (precision != FAME_FP64 && precision != FAME_MIXED) ||
+      (op == FAME_OP_INVAR && (precision != FAME_FP64 || !prm))) {
+    set_err("unsupported operator/precision combination");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if ((op == FAME_OP_QBQ || op == FAME_OP_INVAR) && !c->have_eps) {
+    set_err("permittivity not set");
+    return FAME_ERR_BAD_INPUT;
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    ensure_workspace(c, 1, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), c->cap_mixed, c->cap_vec);
+    if (precision == FAME_MIXED) ensure_workspace(c, 1, c->cap_nstep, c->cap_nwant, true, c->cap_vec);
+    Slot sl;
+    memset(&sl, 0, sizeof(sl));
+    thetas(c->lat, k, sl.th);
+    sl.Nd = reduced_size(c->lat, k);
+    sl.off = c->g.N - sl.Nd;
+    sl.active = 1;
+    if (Nd_out) *Nd_out = sl.Nd;
+    FAME_CK(cudaMemcpyAsync(c->slots.p, &sl, sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
+    Program P(c->stream, false, c->hflag, 100000);
+    Ops o{c, P, 1};
+    const Geom& g = c->g;
+    const long M = 2L * g.N, F = 3L * g.N;
+    const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
+    P.launch(k_tables, dim3((tmax + 255) / 256, 1), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
+             (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
+    if (precision == FAME_FP64) {
+      const double2* x = (const double2*)in;
+      double2* y = (double2*)out;
+      switch (op) {
+        case FAME_OP_QR:
+        case FAME_OP_PR:
+          if (op == FAME_OP_QR)
+            o.plane_inv<double, IN_VEC, false>(x, c->T64.p, 1, M, F, 0);
+          else
+            o.plane_inv<double, IN_VEC, true>(x, c->T64.p, 1, M, F, 0);
+          o.pencil<double, PEN_QR_OUT>(c->T64.p, 1, F, (const double*)nullptr, 0, y);
+          break;
+        case FAME_OP_QRS:
+        case FAME_OP_PRS:
+          o.pencil<double, PEN_QRS_IN>(c->T64.p, 1, F, (const double*)nullptr, 0, nullptr, x);
+          if (op == FAME_OP_QRS)
+            o.plane_fwd<double, EPI_OUT, false>(c->T64.p, y, 1, M, F);
+          else
+            o.plane_fwd<double, EPI_OUT, true>(c->T64.p, y, 1, M, F);
+          break;
+        case FAME_OP_QBQ:
+          o.plane_inv<double, IN_VEC, false>(x, c->T64.p, 1, M, F, 0);
+          o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 0);
+          o.plane_fwd<double, EPI_OUT, false>(c->T64.p, y, 1, M, F);
+          break;
+        case FAME_OP_INVAR: {
+          // one A_r^{-1} apply through the solver's own invAr kernels (U column 0 -> 1)
+          ensure_workspace(c, 1, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), c->cap_mixed, c->cap_vec);
+          const int nstep = c->cap_nstep, nwant = c->cap_nwant;
+          LzArgs L;
+          L.U = c->U.p;
+          L.ustride = M;
+          L.nphys = nstep + 1 + nwant + 1;
+          L.map = c->map.p;
+          L.nstep = nstep;
+          L.nwant = nwant;
+          L.T0 = c->T0.p;
+          L.T1 = c->T1.p;
+          L.h = c->hcoef.p;
+          L.lz = c->lz.p;
+          L.prof = c->prof.p;
+          P.launch(k_lz_init, dim3(1, 1, 1), dim3(256), 0, o.va(Cond{0, c->flags.p + 3}), L);
+          FAME_CK(cudaMemcpyAsync(c->U.p, x, 2L * sl.Nd * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+          SolveCfg s;
+          memset(&s, 0, sizeof(s));
+          s.nslots = 1;
+          s.ls_maxit = prm->ls_maxit;
+          s.ls_tol = prm->ls_tol;
+          s.mixed = 0;
+          const int nvb = vec_blocks(c, 1);
+          Cond cc = P.make_cond(c->flags.p);
+          P.launch(k_invar_pro<false>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), L, 0, c->r64.p, c->x64.p,
+                   (double2*)nullptr, s.ls_tol * s.ls_tol, s.ls_maxit);
+          P.while_loop(cc, [&] {
+            o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p);
+            o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 1);
+            o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
+            P.launch(k_cg_update<double>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
+                     (const double2*)c->p64.p, (const double2*)c->Ap64.p);
+          });
+          P.launch(k_invar_epi<false>, dim3(nvb, 1, 1), dim3(256), 0, o.va(Cond{0, c->flags.p + 3}), L, 0,
+                   (const double2*)c->x64.p);
+          FAME_CK(cudaMemcpyAsync(y, c->U.p + M, 2L * sl.Nd * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+          break;
+        }
+      }
+    } else {
+      const float2* x = (const float2*)in;
+      float2* y = (float2*)out;
+      switch (op) {
+        case FAME_OP_QR:
+        case FAME_OP_PR:
+          if (op == FAME_OP_QR)
+            o.plane_inv<float, IN_VEC, false>(x, c->T32.p, 1, M, F, 0);
+          else
+            o.plane_inv<float, IN_VEC, true>(x, c->T32.p, 1, M, F, 0);
+          o.pencil<float, PEN_QR_OUT>(c->T32.p, 1, F, (const float*)nullptr, 0, y);
+          break;
+        case FAME_OP_QRS:
+        case FAME_OP_PRS:
+          o.pencil<float, PEN_QRS_IN>(c->T32.p, 1, F, (const float*)nullptr, 0, nullptr, x);
+          if (op == FAME_OP_QRS)
+            o.plane_fwd<float, EPI_OUT, false>(c->T32.p, y, 1, M, F);
+          else
+            o.plane_fwd<float, EPI_OUT, true>(c->T32.p, y, 1, M, F);
+          break;
+        case FAME_OP_QBQ:
+          o.plane_inv<float, IN_VEC, false>(x, c->T32.p, 1, M, F, 0);
+          o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 0);
+          o.plane_fwd<float, EPI_OUT, false>(c->T32.p, y, 1, M, F);
+          break;
+      }
+    }
+    FAME_CK(cudaStreamSynchronize(c->stream));
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  } catch (const std::exception& e) {
+    set_err(e.what());
+    return FAME_ERR_WATCHDOG;
+  }
+  return FAME_OK;
+}
+
+int fame_adjoint(fame_ctx* c, const double* freq, const double* evec, int nwant, int host, double* grad_out) {
+  if (!c || !freq || !evec || !grad_out || nwant < 1) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (!c->have_eps) {
+    set_err("permittivity not set");
+    return FAME_ERR_BAD_INPUT;
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    const long N = c->g.N;
+    const double2* E = reinterpret_cast<const double2*>(evec);
+    DBuf<double2> tmp;
+    if (host) {
+      tmp.ensure((size_t)nwant * 3 * N);
+      FAME_CK(cudaMemcpyAsync(tmp.p, evec, (size_t)nwant * 3 * N * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+      E = tmp.p;
+    }
+    DBuf<double> w, den, grad;
+    w.ensure(nwant);
+    den.ensure(nwant);
+    grad.ensure((size_t)nwant * N);
+    FAME_CK(cudaMemcpyAsync(w.p, freq, nwant * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_adj_den<<<nwant, 1024, 0, c->stream>>>(E, c->B64.p, 3 * N, den.p);
+    FAME_CK(cudaGetLastError());
+    k_adj_grad<<<dim3((unsigned)((N + 255) / 256), nwant), 256, 0, c->stream>>>(E, w.p, den.p, N, grad.p);
+    FAME_CK(cudaGetLastError());
+    FAME_CK(cudaMemcpyAsync(grad_out, grad.p, (size_t)nwant * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FAME_CK(cudaStreamSynchronize(c->stream));
+    tmp.release();
+    w.release();
+    den.release();
+    grad.release();
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  return FAME_OK;
+}
+
+}  // extern "C"

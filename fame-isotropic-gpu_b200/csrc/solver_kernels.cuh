@@ -1,0 +1,736 @@
+// CG, invAr and FP64 Lanczos kernels.
+#pragma once
+#include "kernels.cuh"
+
+namespace fame {
+
+// Global index of reduced element i (0 <= i < 2*Nd) to its full frequency index.
+__device__ __forceinline__ int full_index(int i, int Nd, int off) { return (i < Nd ? i : i - Nd) + off; }
+
+struct VecArgs {
+  Geom g;
+  const Slot* slots;
+  const double2* tabs;
+  long vstride;            // per-slot stride of reduced vectors
+  CgState* cg;
+  double* partials;
+  unsigned* counters;      // [nslots] slot tickets, [nslots] grid ticket
+  Cond cond;
+  int nslots;
+};
+
+// ---------------------------------------------------------------- CG update
+// x += a p ; r -= a Ap ; r1 = <r, r>  (FAME_Main/CG.cu:330-341); then beta, the
+// iteration counter and the loop test r1 > tol^2 && k <= maxit (:302).
+template <typename R>
+__global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* x, cplx<R>* r,
+                                                   const cplx<R>* p, const cplx<R>* Ap) {
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  CgState* st = va.cg + slot;
+  const bool live = sl.active && st->active;
+  if (live) {
+    const long b = (long)slot * va.vstride;
+    const int n = 2 * sl.Nd;
+    const R are = (R)st->a_re, aim = (R)st->a_im;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const cplx<R> pp = p[b + i], ap = Ap[b + i];
+      cplx<R> xx = x[b + i], rr = r[b + i];
+      xx.x += are * pp.x - aim * pp.y;
+      xx.y += are * pp.y + aim * pp.x;
+      rr.x -= are * ap.x - aim * ap.y;
+      rr.y -= are * ap.y + aim * ap.x;
+      x[b + i] = xx;
+      r[b + i] = rr;
+      acc[0] += (double)cabs2(rr);
+    }
+    __shared__ double sred[32];
+    block_reduce<1>(acc, sred);
+    double tot[1];
+    if (slot_reduce<1>(acc, va.partials + (size_t)slot * gridDim.x, va.counters + slot, blockIdx.x,
+                       gridDim.x, tot)) {
+      if (threadIdx.x == 0) {
+        st->r0 = st->r1;
+        st->r1 = tot[0];
+        st->beta = st->r1 / st->r0;
+        st->iter++;
+        st->total++;
+        st->active = (st->r1 > st->tol2) && (st->iter <= st->maxit);
+        __threadfence();
+      }
+    }
+  }
+  if (grid_last(va.counters + va.nslots, gridDim.x * gridDim.y * gridDim.z)) {
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int q = 0; q < va.nslots; q++) any |= va.slots[q].active && va.cg[q].active;
+      set_cond(va.cond, any);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- invAr prologue
+// rhs = u / sqrt(Lambda_q) (…invAr.cu:26), CG start x = 0, r = rhs (CG.cu:30-33).
+// Plain FP64 (MIXED = false): r, x are the FP64 CG vectors.  Mixed: b = rhs, y = 0,
+// r64 = b, and the outer refinement loop state is initialised.
+struct LzArgs {
+  double2* U;              // [nslots][nphys][ustride]
+  long ustride;            // column stride (elements)
+  int nphys;
+  int* map;                // [nslots][nstep+1] logical -> physical column
+  int nstep, nwant;
+  double* T0;              // [nslots][nstep]
+  double* T1;              // [nslots][nstep]
+  double* h;               // [nslots][nstep+2] reorthogonalisation coefficients
+  LzState* lz;
+  int* prof;               // [nslots][2]: ls_iter, es_iter (reference Profile counters)
+};
+
+__device__ __forceinline__ double2* ucol(const LzArgs& L, int slot, int logical) {
+  const int ph = L.map[slot * (L.nstep + 1) + logical];
+  return L.U + ((size_t)slot * L.nphys + ph) * L.ustride;
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_invar_pro(VecArgs va, LzArgs L, int j, double2* r64,
+                                                   double2* x64, double2* b64, double tol2, int maxit) {
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  CgState* st = va.cg + slot;
+  const bool live = sl.active && !L.lz[slot].converged;
+  if (live) {
+    const long b = (long)slot * va.vstride;
+    const double2* tab = va.tabs + (size_t)slot * va.g.tab_stride;
+    const double2* u = ucol(L, slot, j);
+    const int Nd = sl.Nd, n = 2 * Nd;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const double s = lq_sqrt_at(va.g, tab, full_index(i, Nd, sl.off));
+      const double2 v = make_double2(u[i].x / s, u[i].y / s);
+      r64[b + i] = v;
+      x64[b + i] = make_double2(0.0, 0.0);
+      if (MIXED) b64[b + i] = v;
+      acc[0] += cabs2(v);
+    }
+    __shared__ double sred[32];
+    block_reduce<1>(acc, sred);
+    double tot[1];
+    if (slot_reduce<1>(acc, va.partials + (size_t)slot * gridDim.x, va.counters + slot, blockIdx.x,
+                       gridDim.x, tot)) {
+      if (threadIdx.x == 0) {
+        if (!MIXED) {
+          st->r1 = tot[0];
+          st->r0 = tot[0];
+          st->r1_0 = tot[0];
+          st->tol2 = tol2;
+          st->iter = 1;
+          st->maxit = maxit;
+          st->active = (tot[0] > tol2) && (1 <= maxit);
+        } else {
+          st->rr = tot[0];
+          st->scale = 1.0 / sqrt(tot[0] > 0 ? tot[0] : 1.0);
+          st->outer = 0;
+          st->outer_max = 40;  // refinement steps per solve; each gains ~5 digits
+          st->total = 0;
+          st->outer_total = 0;
+          st->outer_active = tot[0] > tol2;
+          st->iter = 1;
+          st->active = 0;
+        }
+        __threadfence();
+      }
+    }
+  } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->active = 0;
+    st->outer_active = 0;
+  }
+  if (grid_last(va.counters + va.nslots, gridDim.x * gridDim.y * gridDim.z)) {
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int q = 0; q < va.nslots; q++)
+        any |= va.slots[q].active && (MIXED ? va.cg[q].outer_active : va.cg[q].active);
+      set_cond(va.cond, any);
+    }
+  }
+}
+
+// Start of one FP32 inner solve: r32 = (float)(r64 * scale), x32 = 0; stop when
+// ||r32||^2 <= tau^2 ||r32_0||^2 or after `maxit` products.
+__global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r64, float2* r32,
+                                                   float2* x32, double tau2, int maxit) {
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  CgState* st = va.cg + slot;
+  const bool live = sl.active && st->outer_active;
+  if (live) {
+    const long b = (long)slot * va.vstride;
+    const int n = 2 * sl.Nd;
+    const double sc = st->scale;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const float2 v = make_float2((float)(r64[b + i].x * sc), (float)(r64[b + i].y * sc));
+      r32[b + i] = v;
+      x32[b + i] = make_float2(0.f, 0.f);
+      acc[0] += (double)cabs2(v);
+    }
+    __shared__ double sred[32];
+    block_reduce<1>(acc, sred);
+    double tot[1];
+    if (slot_reduce<1>(acc, va.partials + (size_t)slot * gridDim.x, va.counters + slot, blockIdx.x,
+                       gridDim.x, tot)) {
+      if (threadIdx.x == 0) {
+        st->r1 = tot[0];
+        st->r0 = tot[0];
+        st->r1_0 = tot[0];
+        st->tol2 = tau2 * tot[0];
+        st->iter = 1;
+        st->maxit = maxit;
+        st->active = (tot[0] > st->tol2) && (1 <= maxit);
+        __threadfence();
+      }
+    }
+  } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->active = 0;
+  }
+  if (grid_last(va.counters + va.nslots, gridDim.x * gridDim.y * gridDim.z)) {
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int q = 0; q < va.nslots; q++) any |= va.slots[q].active && va.cg[q].active;
+      set_cond(va.cond, any);
+    }
+  }
+}
+
+// invAr epilogue: w = x / sqrt(Lambda_q) into U[:, j+1] (…invAr.cu:45) and
+// alpha_j = Re<w, u_j> (Lanczos_decomp_gpu.cu:307-309); profile counters
+// (…invAr.cu:41-43: ls_iter += k, es_iter++).
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, const double2* x64) {
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  if (!sl.active || L.lz[slot].converged) return;
+  const long b = (long)slot * va.vstride;
+  const double2* tab = va.tabs + (size_t)slot * va.g.tab_stride;
+  const double2* u = ucol(L, slot, j);
+  double2* w = ucol(L, slot, j + 1);
+  const int Nd = sl.Nd, n = 2 * Nd;
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double s = lq_sqrt_at(va.g, tab, full_index(i, Nd, sl.off));
+    const double2 v = make_double2(x64[b + i].x / s, x64[b + i].y / s);
+    w[i] = v;
+    acc[0] += v.x * u[i].x + v.y * u[i].y;
+  }
+  __shared__ double sred[32];
+  block_reduce<1>(acc, sred);
+  double tot[1];
+  if (slot_reduce<1>(acc, va.partials + (size_t)slot * gridDim.x, va.counters + slot, blockIdx.x,
+                     gridDim.x, tot)) {
+    if (threadIdx.x == 0) {
+      L.T0[slot * L.nstep + j] = tot[0];
+      const CgState* st = va.cg + slot;
+      L.prof[slot * 2 + 0] += MIXED ? st->total : st->iter;
+      L.prof[slot * 2 + 1] += 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- Lanczos step
+// w' = w - alpha_j u_j - beta_{j-1} u_{j-1}; ||w'||^2 and, for j >= 1, the
+// coefficients <u_i, w'> (i <= j) of one classical Gram-Schmidt pass.  The
+// reference normalises first and then runs one modified Gram-Schmidt pass
+// without renormalising (Lanczos_decomp_gpu.cu:311-329); both leave u_{j+1}
+// orthogonal to the basis to rounding level.
+constexpr int kLzRows = 2048;  // rows per CTA, staged in shared memory (32 KB)
+
+__global__ void __launch_bounds__(256) k_lz_dots(VecArgs va, LzArgs L, int j) {
+  __shared__ double2 wsh[kLzRows];
+  __shared__ double red[(2 * 64 + 1) * 8];  // [value][warp]
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  if (!sl.active || L.lz[slot].converged) return;
+  const int n = 2 * sl.Nd;
+  const int r0 = blockIdx.x * kLzRows;
+  const int rows = min(kLzRows, n - r0);
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const double al = L.T0[slot * L.nstep + j];
+  const double be = j > 0 ? L.T1[slot * L.nstep + j - 1] : 0.0;
+  const double2* w = ucol(L, slot, j + 1);
+  const double2* uj = ucol(L, slot, j);
+  const double2* ujm = j > 0 ? ucol(L, slot, j - 1) : uj;
+  const int nval = 1 + (j > 0 ? 2 * (j + 1) : 0);
+  double nrm = 0.0;
+  for (int q = threadIdx.x; q < rows; q += blockDim.x) {
+    const int i = r0 + q;
+    double2 v = w[i];
+    v.x -= al * uj[i].x + be * ujm[i].x;
+    v.y -= al * uj[i].y + be * ujm[i].y;
+    wsh[q] = v;
+    nrm += cabs2(v);
+  }
+  for (int o = 16; o > 0; o >>= 1) nrm += __shfl_down_sync(0xffffffffu, nrm, o);
+  if (lane == 0) red[0 * 8 + wid] = nrm;
+  __syncthreads();
+  if (j > 0) {
+    for (int c = 0; c <= j; c++) {
+      const double2* u = ucol(L, slot, c);
+      double dr = 0.0, di = 0.0;
+      for (int q = threadIdx.x; q < rows; q += blockDim.x) {
+        const double2 a = u[r0 + q], b = wsh[q];
+        dr += a.x * b.x + a.y * b.y;  // conj(u) w'
+        di += a.x * b.y - a.y * b.x;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        dr += __shfl_down_sync(0xffffffffu, dr, o);
+        di += __shfl_down_sync(0xffffffffu, di, o);
+      }
+      if (lane == 0) {
+        red[(1 + 2 * c) * 8 + wid] = dr;
+        red[(2 + 2 * c) * 8 + wid] = di;
+      }
+    }
+  }
+  __syncthreads();
+  // per-CTA partials in global memory, last CTA of the slot sums them in order
+  double* part = va.partials + (size_t)slot * gridDim.x * (2 * 64 + 1);
+  for (int v = threadIdx.x; v < nval; v += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < nw; q++) s += red[v * 8 + q];
+    part[(size_t)blockIdx.x * (2 * 64 + 1) + v] = s;
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(va.counters + slot, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int v = threadIdx.x; v < nval; v += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < (int)gridDim.x; q++) s += *((volatile double*)&part[(size_t)q * (2 * 64 + 1) + v]);
+    red[v] = s;  // reuse (no other warps read red any more)
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double beta = sqrt(red[0]);
+    L.T1[slot * L.nstep + j] = beta;
+    double* h = L.h + (size_t)slot * 2 * (L.nstep + 2);
+    for (int v = 1; v < nval; v++) h[v - 1] = red[v];
+    va.counters[slot] = 0u;
+  }
+}
+
+// u_{j+1} = (w' - sum_i <u_i, w'> u_i) / beta_j
+__global__ void __launch_bounds__(256) k_lz_update(VecArgs va, LzArgs L, int j) {
+  __shared__ double2 hs[64];
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  if (!sl.active || L.lz[slot].converged) return;
+  const int n = 2 * sl.Nd;
+  const double beta = L.T1[slot * L.nstep + j];
+  const double inv = 1.0 / beta;
+  const double al = L.T0[slot * L.nstep + j];
+  const double be = j > 0 ? L.T1[slot * L.nstep + j - 1] : 0.0;
+  const double* h = L.h + (size_t)slot * 2 * (L.nstep + 2);
+  if (j > 0)
+    for (int c = threadIdx.x; c <= j; c += blockDim.x) hs[c] = make_double2(h[2 * c], h[2 * c + 1]);
+  __syncthreads();
+  double2* w = ucol(L, slot, j + 1);
+  const double2* uj = ucol(L, slot, j);
+  const double2* ujm = j > 0 ? ucol(L, slot, j - 1) : uj;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 v = w[i];
+    v.x -= al * uj[i].x + be * ujm[i].x;
+    v.y -= al * uj[i].y + be * ujm[i].y;
+    if (j > 0) {
+      for (int c = 0; c <= j; c++) {
+        const double2 u = ucol(L, slot, c)[i];
+        const double2 hc = hs[c];
+        v.x -= hc.x * u.x - hc.y * u.y;
+        v.y -= hc.x * u.y + hc.y * u.x;
+      }
+    }
+    w[i] = make_double2(v.x * inv, v.y * inv);
+  }
+}
+
+// e_M start vector (Lanczos_decomp_gpu.cu:93-107) and map/pool initialisation.
+__global__ void k_lz_init(VecArgs va, LzArgs L) {
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  if (blockIdx.x == 0 && threadIdx.x <= L.nstep) L.map[slot * (L.nstep + 1) + threadIdx.x] = threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x <= L.nwant)
+    L.map[va.nslots * (L.nstep + 1) + slot * (L.nwant + 1) + threadIdx.x] = L.nstep + 1 + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    L.lz[slot].converged = 0;
+    L.lz[slot].restarts = 0;
+    L.lz[slot].nconv = 0;
+    L.prof[slot * 2] = 0;
+    L.prof[slot * 2 + 1] = 0;
+  }
+  if (!sl.active) return;
+  double2* u = L.U + (size_t)slot * L.nphys * L.ustride;  // physical column 0 == logical 0
+  const int n = 2 * sl.Nd;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    u[i] = make_double2(i == n - 1 ? 1.0 : 0.0, 0.0);
+}
+
+// ---------------------------------------------------------------- tridiagonal stage
+// One warp per slot.  (1) Eigen-decomposition of the symmetric tridiagonal T
+// (diag T0, off-diag T1) by the implicit QL method with Wilkinson shifts (Bowdler,
+// Martin, Reinsch and Wilkinson, "The QR and QL algorithms for symmetric matrices",
+// Numer. Math. 11, 1968), eigenvalues sorted in descending order as zpteqr returns
+// them (Lanczos_Isotropic.cu:53).  (2) The convergence test of Lanczos_Isotropic.cu:58-72.
+// (3) If not converged: the lock/purge restart of Lanczos_LockPurge_gpu.cu:7-48
+// (exact shifts = unwanted Ritz values, GVqrrq_g steps, :95-190), applied to an
+// identity matrix G of order nstep+1 instead of to U, so that U is updated later by
+// one product U*G[:, 0..nwant].
+constexpr int kMaxStep = 64;
+
+struct TriArgs {
+  LzArgs L;
+  const Slot* slots;
+  double* theta;   // [nslots][nstep] Ritz values (descending)
+  double* Z;       // [nslots][nstep*nstep] eigenvectors, column-major (z[r + c*nstep])
+  double* G;       // [nslots][(nstep+1)*(nwant+1)] restart transform, column-major
+  double tol;
+  int maxit;
+  Cond cond;       // "some slot needs another restart"
+  int nslots;
+  int* status;     // [nslots] 0 ok, 2 no convergence, 3 QL failure
+  unsigned* ctr;   // grid ticket counter
+};
+
+// dynamic shared memory of k_tridiag for nstep = n
+inline size_t tridiag_smem(int n) {
+  return sizeof(double) * ((size_t)n * n + (size_t)(n + 1) * (n + 1) + 8 * (size_t)n) + sizeof(int) * n;
+}
+
+__device__ void givens_ref(double a, double b, double& c, double& s, double& r) {
+  // given_rotation (Lanczos_LockPurge_gpu.cu:245-265)
+  double t, u;
+  if (fabs(a) > fabs(b)) {
+    t = b / a;
+    u = (fabs(a) / a) * sqrt(1 + t * t);
+    c = 1.0 / u;
+    s = c * t;
+    r = a * u;
+    s = -s;
+  } else {
+    t = a / b;
+    u = (fabs(b) / b) * sqrt(1 + t * t);
+    s = 1.0 / u;
+    c = s * t;
+    r = b * u;
+    s = -s;
+  }
+}
+
+__global__ void __launch_bounds__(32) k_tridiag(TriArgs a) {
+  extern __shared__ __align__(16) double tsm[];
+  const LzArgs& L = a.L;
+  const int n = L.nstep, nw = L.nwant, lane = threadIdx.x;
+  double* Zs = tsm;                       // n*n
+  double* Gs = Zs + n * n;                // (n+1)^2
+  double* d = Gs + (n + 1) * (n + 1);     // 8 vectors of n
+  double* e = d + n;
+  double* T0 = e + n;
+  double* T1 = T0 + n;
+  double* T2 = T1 + n;
+  double* T3 = T2 + n;
+  double* cc = T3 + n;
+  double* ss = cc + n;
+  int* order = reinterpret_cast<int*>(ss + n);
+  __shared__ int fail;
+  const int slot = blockIdx.x;
+  LzState* lz = L.lz + slot;
+  const bool live = a.slots[slot].active && !lz->converged;
+  if (live) {
+    for (int i = lane; i < n; i += 32) {
+      d[i] = L.T0[slot * n + i];
+      e[i] = i < n - 1 ? L.T1[slot * n + i] : 0.0;
+      T0[i] = d[i];
+      T1[i] = L.T1[slot * n + i];
+    }
+    for (int i = lane; i < n * n; i += 32) Zs[i] = (i % (n + 1)) == 0 ? 1.0 : 0.0;  // Z[r + c*n]
+    if (lane == 0) fail = 0;
+    __syncwarp();
+    // ---- implicit QL; lane 0 runs the scalar recurrence, all lanes rotate Z rows
+    for (int l = 0; l < n; l++) {
+      int iter = 0;
+      while (true) {
+        int m = l;
+        for (; m < n - 1; m++) {
+          const double dd = fabs(d[m]) + fabs(d[m + 1]);
+          if (fabs(e[m]) <= 1e-300 || fabs(e[m]) + dd == dd) break;
+        }
+        if (m == l) break;
+        if (++iter > 60) {
+          if (lane == 0) fail = 1;
+          break;
+        }
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g >= 0 ? fabs(r) : -fabs(r)));
+        double s = 1.0, c = 1.0, p = 0.0;
+        int i = m - 1;
+        bool underflow = false;
+        for (; i >= l; i--) {
+          const double f = s * e[i], b = c * e[i];
+          r = hypot(f, g);
+          __syncwarp();
+          if (lane == 0) e[i + 1] = r;
+          if (r == 0.0) {
+            __syncwarp();
+            if (lane == 0) {
+              d[i + 1] -= p;
+              e[m] = 0.0;
+            }
+            underflow = true;
+            __syncwarp();
+            break;
+          }
+          s = f / r;
+          c = g / r;
+          g = d[i + 1] - p;
+          r = (d[i] - g) * s + 2.0 * c * b;
+          p = s * r;
+          __syncwarp();
+          if (lane == 0) d[i + 1] = g + p;
+          g = c * r - b;
+          for (int k = lane; k < n; k += 32) {
+            const double fz = Zs[k + (i + 1) * n];
+            Zs[k + (i + 1) * n] = s * Zs[k + i * n] + c * fz;
+            Zs[k + i * n] = c * Zs[k + i * n] - s * fz;
+          }
+          __syncwarp();
+        }
+        if (underflow) continue;
+        __syncwarp();
+        if (lane == 0) {
+          d[l] -= p;
+          e[l] = g;
+          e[m] = 0.0;
+        }
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+    // ---- sort descending (selection on lane 0; n <= 64)
+    if (lane == 0) {
+      for (int i = 0; i < n; i++) order[i] = i;
+      for (int i = 0; i < n; i++) {
+        int best = i;
+        for (int k = i + 1; k < n; k++)
+          if (d[order[k]] > d[order[best]]) best = k;
+        const int t = order[i];
+        order[i] = order[best];
+        order[best] = t;
+      }
+    }
+    __syncwarp();
+    double* th = a.theta + (size_t)slot * n;
+    double* Zg = a.Z + (size_t)slot * n * n;
+    for (int i = lane; i < n; i += 32) th[i] = d[order[i]];
+    for (int q = lane; q < n * n; q += 32) {
+      const int r = q % n, c = q / n;
+      Zg[q] = Zs[r + order[c] * n];
+    }
+    __syncwarp();
+    // ---- convergence (Lanczos_Isotropic.cu:58-72): |beta_last * z(last, i)| < tol
+    int conv = 0;
+    if (lane == 0) {
+      const double bl = L.T1[slot * n + n - 1];
+      for (int i = 0; i < nw; i++) {
+        const double res = bl * fabs(Zs[(n - 1) + order[i] * n]);
+        if (res < a.tol) conv++;
+        else break;
+      }
+      lz->nconv = conv;
+      if (fail) a.status[slot] = 3;
+    }
+    conv = __shfl_sync(0xffffffffu, conv, 0);
+    const bool done = conv == nw || fail;
+    if (done) {
+      if (lane == 0) lz->converged = 1;
+    } else if (lz->restarts >= a.maxit) {
+      if (lane == 0) {
+        lz->converged = 1;
+        a.status[slot] = 2;
+      }
+    } else {
+      // ---- lock & purge on G (order nstep+1)
+      const int n1 = n + 1;
+      for (int q = lane; q < n1 * n1; q += 32) Gs[q] = (q % (n1 + 1)) == 0 ? 1.0 : 0.0;
+      __syncwarp();
+      for (int jj0 = 0; jj0 < n - nw; jj0++) {
+        const int nn = n - jj0;
+        const double shift = d[order[nw + jj0]];
+        if (lane == 0) {
+          // GVqrrq_g(T0, T1, T2, T3, c, s, shift, nn)
+          for (int i = 0; i < nn - 1; i++) T3[i] = T1[i];
+          for (int i = 0; i < nn; i++) T0[i] -= shift;
+          for (int i = 0; i < nn - 1; i++) {
+            double ci, si, r;
+            givens_ref(T0[i], T1[i], ci, si, r);
+            cc[i] = ci;
+            ss[i] = si;
+            T0[i] = r;
+            T1[i] = 0.0;
+            const double aa = T3[i], bb = T0[i + 1];
+            T3[i] = ci * aa - si * bb;
+            T0[i + 1] = si * aa + ci * bb;
+            if (i < nn - 2) {
+              T2[i] = -si * T3[i + 1];
+              T3[i + 1] = ci * T3[i + 1];
+            }
+          }
+          double R0 = T0[0], R1 = T3[0], R2 = T1[0], R3 = T0[1];
+          T0[0] = cc[0] * R0 - ss[0] * R1;
+          T3[0] = ss[0] * R0 + cc[0] * R1;
+          T1[0] = cc[0] * R2 - ss[0] * R3;
+          T0[1] = ss[0] * R2 + cc[0] * R3;
+          for (int i = 1; i < nn - 1; i++) {
+            const double q0 = T3[i - 1], q1 = T2[i - 1], q2 = T0[i], q3 = T3[i], q4 = T1[i], q5 = T0[i + 1];
+            T3[i - 1] = cc[i] * q0 - ss[i] * q1;
+            T2[i - 1] = ss[i] * q0 + cc[i] * q1;
+            T0[i] = cc[i] * q2 - ss[i] * q3;
+            T3[i] = ss[i] * q2 + cc[i] * q3;
+            T1[i] = cc[i] * q4 - ss[i] * q5;
+            T0[i + 1] = ss[i] * q4 + cc[i] * q5;
+          }
+          for (int i = 0; i < nn - 1; i++) T1[i] = (T1[i] + T3[i]) / 2.0;
+          for (int i = 0; i < nn; i++) T0[i] += shift;
+          // the final rotation couples column nn-1 with the residual column nn:
+          // (c, s) = (T1[nn-2], s[nn-2] * T1[nn-1]) (Lanczos_LockPurge_gpu.cu:30-31)
+          ss[nn - 1] = ss[nn - 2] * T1[nn - 1];
+          cc[nn - 1] = T1[nn - 2];
+        }
+        __syncwarp();
+        // Zdrot(U[:, jj+1], U[:, jj], c, s) for jj < nn-1, then (c, s) = (T1[nn-2], s[nn-2]*T1[nn-1])
+        for (int jj = 0; jj < nn; jj++) {
+          const double c = cc[jj];
+          const double s = ss[jj];
+          for (int r = lane; r < n1; r += 32) {
+            const double x = Gs[r + (jj + 1) * n1], y = Gs[r + jj * n1];
+            Gs[r + (jj + 1) * n1] = c * x + s * y;
+            Gs[r + jj * n1] = -s * x + c * y;
+          }
+          __syncwarp();
+        }
+        // normalise column nn-1, purge T0/T1[nn-1] and column nn
+        double nrm = 0.0;
+        for (int r = lane; r < n1; r += 32) nrm += Gs[r + (nn - 1) * n1] * Gs[r + (nn - 1) * n1];
+        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+        nrm = sqrt(nrm);
+        for (int r = lane; r < n1; r += 32) {
+          Gs[r + (nn - 1) * n1] /= nrm;
+          Gs[r + nn * n1] = 0.0;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          T1[nn - 2] = nrm;
+          T0[nn - 1] = 0.0;
+          T1[nn - 1] = 0.0;
+        }
+        __syncwarp();
+      }
+      double* Gg = a.G + (size_t)slot * n1 * (nw + 1);
+      for (int q = lane; q < n1 * (nw + 1); q += 32) Gg[q] = Gs[q];
+      for (int i = lane; i < n; i += 32) {
+        L.T0[slot * n + i] = T0[i];
+        L.T1[slot * n + i] = T1[i];
+      }
+      if (lane == 0) lz->restarts++;
+    }
+  }
+  __syncwarp();
+  // grid-wide "any slot still restarting" (gridDim.x == nslots, one warp each)
+  __shared__ bool last;
+  __threadfence();
+  if (lane == 0) last = atomicAdd(a.ctr, 1u) == (unsigned)gridDim.x - 1;
+  __syncwarp();
+  if (last && lane == 0) {
+    __threadfence();
+    *a.ctr = 0u;
+    int any = 0;
+    for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && !a.L.lz[q].converged;
+    set_cond(a.cond, any);
+  }
+}
+
+// ---------------------------------------------------------------- U * G products
+// out[:, c] = sum_r U[:, map[r]] * G[r, c] for c < ncols (G real, column-major,
+// leading dimension ldg).  Used for the restart (lock/purge) and for the Ritz
+// vectors ev = U(:, 0:nstep) z(:, 0:nwant) (Lanczos_Isotropic.cu:93).
+// mode 0: restart (writes into the free physical columns, then remaps)
+// mode 1: Ritz vectors into `out` ([slot][ncols][ustride])
+template <int CH>
+__global__ void __launch_bounds__(256) k_ugemm(VecArgs va, LzArgs L, const double* G, int ldg, int nrows,
+                                               int ncols, int mode, double2* out, int c0) {
+  const int slot = blockIdx.z;
+  const Slot sl = va.slots[slot];
+  if (!sl.active) return;
+  if (mode == 0 && L.lz[slot].converged) return;
+  __shared__ double Gs[(kMaxStep + 1) * CH];
+  __shared__ int cols[kMaxStep + 1];
+  const double* Gg = G + (size_t)slot * ldg * (mode == 0 ? (L.nwant + 1) : L.nstep);
+  const int nc = min(CH, ncols - c0);
+  for (int q = threadIdx.x; q < nrows * nc; q += blockDim.x) {
+    const int r = q % nrows, c = q / nrows;
+    Gs[r + c * nrows] = Gg[r + (c0 + c) * ldg];
+  }
+  for (int r = threadIdx.x; r < nrows; r += blockDim.x) cols[r] = L.map[slot * (L.nstep + 1) + r];
+  __syncthreads();
+  const int n = 2 * sl.Nd;
+  const double2* U = L.U + (size_t)slot * L.nphys * L.ustride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 acc[CH];
+#pragma unroll
+    for (int c = 0; c < CH; c++) acc[c] = make_double2(0.0, 0.0);
+    for (int r = 0; r < nrows; r++) {
+      const double2 u = U[(size_t)cols[r] * L.ustride + i];
+#pragma unroll
+      for (int c = 0; c < CH; c++) {
+        const double gv = Gs[r + c * nrows];
+        acc[c].x += gv * u.x;
+        acc[c].y += gv * u.y;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+      if (c < nc) {
+        double2* dst;
+        if (mode == 0) {
+          // free physical column: the pool entries after the logical map
+          const int ph = L.map[va.nslots * (L.nstep + 1) + slot * (L.nwant + 1) + c0 + c];
+          dst = L.U + ((size_t)slot * L.nphys + ph) * L.ustride;
+        } else {
+          dst = out + ((size_t)slot * ncols + c0 + c) * L.ustride;
+        }
+        dst[i] = acc[c];
+      }
+    }
+  }
+}
+
+// After the restart product: logical 0..nwant -> the former free columns; the old
+// columns become the new pool (first nstep-nwant reused as logical nwant+1..nstep).
+__global__ void k_remap(LzArgs L, const Slot* slots, int nslots) {
+  const int slot = blockIdx.x;
+  if (threadIdx.x != 0 || !slots[slot].active || L.lz[slot].converged) return;
+  int* mp = L.map + slot * (L.nstep + 1);
+  int* pool = L.map + nslots * (L.nstep + 1) + slot * (L.nwant + 1);
+  int old[kMaxStep + 1], fr[kMaxStep + 1];
+  for (int c = 0; c <= L.nstep; c++) old[c] = mp[c];
+  for (int c = 0; c <= L.nwant; c++) fr[c] = pool[c];
+  for (int c = 0; c <= L.nwant; c++) mp[c] = fr[c];
+  const int rest = L.nstep - L.nwant;
+  for (int c = 0; c < rest; c++) mp[L.nwant + 1 + c] = old[c];
+  for (int c = 0; c <= L.nwant; c++) pool[c] = old[rest + c];
+}
+
+}  // namespace fame

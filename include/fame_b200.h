@@ -1,0 +1,142 @@
+/*
+ * fame_b200.h -- C ABI of the B200-native band-structure path of FAME-Isotropic-GPU.
+ *
+ * One shared library (fame-isotropic-gpu_b200/libfame_b200.so) exports these
+ * symbols with C linkage.  Signatures use plain pointers and sizes only.  Every
+ * entry point returns an int status (FAME_OK = 0) and never exits or asserts;
+ * fame_last_error() returns a message for the calling thread's last failure.
+ *
+ * Conventions shared with the reference (relative to its project root):
+ *   - grid (Nx, Ny, Nz) is the reference's adjusted grid (FAME_Preprocessing/
+ *     FAME_Parameter_Generator.cpp:106-112), N = Nx*Ny*Nz;
+ *   - edge permittivities B are 3N doubles, x-, y-, z-edge blocks, index
+ *     i + Nx*(j + Ny*k) (FAME_Main/FAME_Matrix_B_Isotropic.cu:4-74);
+ *   - wave vectors are Cartesian without the 2*pi factor, in the computational
+ *     frame (FAME_Main/FAME_Matrix_Lambdas.cu:43-45);
+ *   - eigenvectors E are 3N complex128 per band, stored as (re, im) pairs, band
+ *     major, scaled like the reference's Eigen_Restoration_Isotropic
+ *     (FAME_Main/FAME_Fast_Algorithms_Isotropic.cu:90-125).
+ */
+#ifndef FAME_B200_H
+#define FAME_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FAME_OK = 0,
+  FAME_ERR_BAD_INPUT = 1,
+  FAME_ERR_NO_CONVERGENCE = 2,
+  FAME_ERR_WATCHDOG = 3,
+  FAME_ERR_CUDA = 4,
+  FAME_ERR_NO_DEVICE = 5,
+  FAME_ERR_UNSUPPORTED = 6
+};
+
+/* precision modes */
+enum { FAME_FP64 = 0, FAME_MIXED = 1 };
+
+/* operators for fame_apply (device pointers, one k-point) */
+enum {
+  FAME_OP_QR = 0,   /* y(3N) = Q_r x(2Nd)     FAME_Matrix_Vector_Production_Qr.cu:8-78  */
+  FAME_OP_QRS = 1,  /* y(2Nd) = Q_r^* x(3N)   FAME_Matrix_Vector_Production_Qrs.cu:7-58 */
+  FAME_OP_QBQ = 2,  /* y(2Nd) = Q_r^* B^-1 Q_r x   …Isotropic_QBQ.cu:8-67              */
+  FAME_OP_PR = 3,   /* y(3N) = P_r x(2Nd)     FAME_Matrix_Vector_Production_Pr.cu:11-104 */
+  FAME_OP_PRS = 4,  /* y(2Nd) = P_r^* x(3N)   FAME_Matrix_Vector_Production_Prs.cu:9-58 */
+  FAME_OP_INVAR = 5 /* y(2Nd) = A_r^-1 x      …Isotropic_invAr.cu:8-48 (CG inside)    */
+};
+
+typedef struct fame_ctx fame_ctx;
+
+/* Lattice of the computation.  Replaces the grid / lattice part of the reference's
+ * PAR struct (include/FAME_Internal_Common.h:64-99,179-187). */
+typedef struct {
+  int grid[3];              /* Nx, Ny, Nz */
+  double mesh_len[3];       /* hx, hy, hz (Par.mesh.mesh_len) */
+  double lattice_vec_a[9];  /* computational-frame a1, a2, a3 (Par.lattice.lattice_vec_a) */
+  int simple;               /* 1: simple_cubic / primitive_orthorhombic / primitive_tetragonal */
+  int m[4];                 /* m1..m4 boundary shifts (General lattices) */
+  double t1[3];             /* boundary translation t1 (General lattices) */
+} fame_lattice;
+
+/* Solver parameters (the reference's ES and LS, include/FAME_Internal_Common.h:157-167). */
+typedef struct {
+  int nwant;        /* ES.nwant */
+  int nstep;        /* ES.nstep (<= 64) */
+  int es_maxit;     /* ES.maxit: maximum Lanczos restarts */
+  double es_tol;    /* ES.tol: |beta_m z_m,i| < tol */
+  int ls_maxit;     /* LS.maxit */
+  double ls_tol;    /* LS.tol: absolute ||r|| of the inner solve */
+  int precision;    /* FAME_FP64 or FAME_MIXED */
+  int batch;        /* k-points in flight per launch (0 = automatic) */
+  int use_graph;    /* 1 = run each batch as one CUDA graph (default), 0 = host-driven loop */
+  double inner_tol; /* FAME_MIXED: relative tolerance of each FP32 inner solve (0 = 1e-5) */
+  int inner_maxit;  /* FAME_MIXED: products per FP32 inner solve (0 = 200) */
+  int want_vectors; /* 1 = compute and return the eigenvectors E */
+} fame_solver_params;
+
+/* Per k-point counters (the reference's PROFILE, include/FAME_Internal_Common.h:205-211,
+ * plus the mixed-precision breakdown). */
+typedef struct {
+  int ls_iter;      /* Profile.ls_iter: CG products (reference counting, CG.cu:301,342) */
+  int es_iter;      /* Profile.es_iter: A_r^-1 applications */
+  int restarts;     /* Lanczos restarts */
+  int status;       /* FAME_OK / FAME_ERR_NO_CONVERGENCE for this k */
+  int Nd;           /* N or N-1 (Gamma point) */
+  int pad;
+} fame_kcounters;
+
+/* Create a context on `device` for one lattice/grid.  Allocates nothing per k yet. */
+int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out);
+void fame_ctx_destroy(fame_ctx* ctx);
+
+/* Edge permittivities B (3N doubles, host).  Replaces FAME_Matrix_B_Isotropic's
+ * output (FAME_Main/FAME_Matrix_B_Isotropic.cu:4-74). */
+int fame_set_eps(fame_ctx* ctx, const double* B_eps);
+
+/* B from the reference's material index map Binout (3 * material_num * N ints,
+ * FAME_Preprocessing/FAME_Material_Locate_Index.cpp:101-113) with the same
+ * last-material-wins rule as FAME_Matrix_B_Isotropic.cu:100-131. */
+int fame_set_material(fame_ctx* ctx, const int* binout, int material_num, const double* eps_in,
+                      double eps_out);
+
+/* Solve nk k-points (k_xyz: 3*nk doubles).  Outputs (host, caller owned):
+ *   freq_out   nk*nwant   omega = sqrt(1/theta) per band (FAME_Fast_Algorithms_Isotropic.cu
+ *                         + Lanczos_Isotropic.cu:88, Gamma patch :61-79);
+ *   relres_out nk*nwant   ||C^H C E - w^2 B E|| / (w^2 ||B E||) evaluated in FP64, or NULL;
+ *   relerr_out nk*nwant   |w^2 - rho| / rho with rho the FP64 Rayleigh quotient, or NULL;
+ *   evec_out   nk*nwant*3N complex128 (params->want_vectors), or NULL;
+ *   counters   nk entries, or NULL.
+ * Replaces FAME_Fast_Algorithms_Driver (FAME_Main/FAME_Main_Code.cu:142-171) over
+ * the k-loop of FAME_Main_Code (:79-133). */
+int fame_solve_kpoints(fame_ctx* ctx, const double* k_xyz, int nk, const fame_solver_params* params,
+                       double* freq_out, double* relres_out, double* relerr_out, double* evec_out,
+                       fame_kcounters* counters);
+
+/* Apply one operator at one k-point on device buffers (complex, interleaved):
+ * in/out are device pointers of length given in the FAME_OP_* comments.
+ * precision: FAME_FP64 (complex128 buffers) or FAME_MIXED (complex64 buffers, not
+ * for FAME_OP_INVAR).  For FAME_OP_INVAR ls_tol / ls_maxit come from `params`.
+ * Returns Nd through *Nd_out when not NULL. */
+int fame_apply(fame_ctx* ctx, int op, const double* k_xyz, const void* in, void* out, int precision,
+               const fame_solver_params* params, int* Nd_out);
+
+/* Hellmann-Feynman adjoint for the isotropic problem C^H C E = w^2 B E:
+ * dw_i/dB_e = -(w_i/2) |E_i,e|^2 / (E_i^H B E_i) for every edge e, summed over the
+ * three edges of each voxel (B_x = B_y = B_z = eps per voxel).  evec is the
+ * device or host array returned by fame_solve_kpoints for one k (nwant*3N complex128),
+ * `host` tells which.  grad_out: nwant*N doubles (host). */
+int fame_adjoint(fame_ctx* ctx, const double* freq, const double* evec, int nwant, int host,
+                 double* grad_out);
+
+/* Grid size N and maximum reduced size 2N of the context, for buffer sizing. */
+int fame_ctx_sizes(const fame_ctx* ctx, long long* N_out);
+
+const char* fame_last_error(void);
+const char* fame_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FAME_B200_H */

@@ -3,15 +3,16 @@
     python tests/golden/make_golden.py pre            # CPU, needs the reference sources
     python tests/golden/make_golden.py ref OUTDIR     # on a B200, runs the reference's
                                                       # FP64 CUDA solver (oracle/_ref)
+    python tests/golden/make_golden.py condense OUTDIR
 
 `pre` runs the reference's preprocessing (FAME_Preprocessing) through
 oracle/_ref/fame_ref_harness for every named workload and stores its integer and
 geometric outputs (grid, m1-m4, Omega, k path, Binout, ...) as <name>_pre.npz.
 
-`ref` runs the reference's FP64 solver on the small workloads and on the 96^3
-metric workload's first k-points, writing <name>_ref.json (frequencies, counters)
-and <name>_apply.npz (reference Qr/Qrs/QBQ/invAr applied to seeded vectors).
-The outputs are copied into tests/golden/ by hand after the run.
+`ref` runs the reference's FP64 solver on the small workloads and on the full 96^3
+metric band path, writing <name>_ref.jsonl (frequencies, counters, wall time per k)
+and <name>_apply.npz (reference Qr/Qrs/QBQ/invAr applied to seeded vectors) into
+OUTDIR; `condense OUTDIR` then writes the committed subset into tests/golden/.
 """
 from __future__ import annotations
 
@@ -66,8 +67,8 @@ REF_RUNS = [
     ("fcc16", None),
     ("bcc12", None),
     ("hex12", None),
-    ("sc32", "0,1,3"),
-    ("sc96", "0,1"),
+    ("sc32", None),
+    ("sc96", None),
 ]
 
 
@@ -109,10 +110,38 @@ def do_ref(outdir):
         print("done", name)
 
 
+
+
+def condense(src, dst=GOLDEN):
+    """Keeps the committed part of a `ref` run: all frequencies and counters, and
+    the operator applications at k-points 0 (Gamma) and 1 only."""
+    meta = open(os.path.join(src, "gpu.txt")).read().strip().splitlines()
+    for name, _ in REF_RUNS:
+        recs = [json.loads(l) for l in open(os.path.join(src, f"{name}_ref.jsonl"))]
+        out = dict(workload=name, device=meta[1].split(",")[0], host_cores=int(meta[2]),
+                   note="reference FP64 CUDA build (oracle/_ref/fame_ref_harness solve), "
+                        "es_tol=ls_tol=1e-10, es_maxit=100, ls_maxit=1000",
+                   kpoints=[dict(k=r["k"], wave_vec=r["wave_vec"], Nd=r["Nd"], freq=r["freq"],
+                                 ls_iter=r["ls_iter"], es_iter=r["es_iter"], wall_s=r["wall_s"])
+                            for r in recs])
+        with open(os.path.join(dst, f"{name}_ref.json"), "w") as f:
+            json.dump(out, f, indent=1)
+        ap = os.path.join(src, f"{name}_apply.npz")
+        if os.path.exists(ap):
+            z = np.load(ap)
+            keep = {"x": z["x"]}
+            for k in (0, 1):
+                for key in ("Qr", "Qrs", "QBQ", "invAr", "Nd"):
+                    keep[f"{key}_{k}"] = z[f"{key}_{k}"]
+            np.savez_compressed(os.path.join(dst, f"{name}_apply.npz"), **keep)
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "pre":
         do_pre()
     elif sys.argv[1] == "ref":
         do_ref(sys.argv[2])
+    elif sys.argv[1] == "condense":
+        condense(sys.argv[2])
     else:
         raise SystemExit(__doc__)

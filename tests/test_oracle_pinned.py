@@ -1,0 +1,79 @@
+"""Pins the numpy oracle (oracle/fame_oracle.py) to the reference itself.
+
+* integer maps: Binout from the oracle's material-locate restatement equals the
+  reference preprocessing output bit for bit (all four lattice families);
+* operators: Q_r, Q_r^*, Q_r^* B^-1 Q_r and A_r^-1 equal the reference's FP64
+  CUDA build on the same seeded vectors (tests/golden/*_apply.npz, produced by
+  tests/golden/make_golden.py on a B200);
+* frequencies: a full oracle solve reproduces the reference's eigenvalues.
+"""
+import numpy as np
+import pytest
+
+import fame_oracle as fo
+from fixtures import edge_eps, load_apply, load_pre, load_ref
+
+APPLY = ["sc16", "fcc16", "bcc12", "hex12"]
+
+
+@pytest.mark.parametrize("name", ["sc16", "sc32", "fcc16", "bcc12", "hex12", "bcc48", "fcc64"])
+def test_binout_bit_exact(name):
+    par = load_pre(name)
+    b = fo.material_locate(par, par["material"])
+    assert b.dtype == np.int32
+    assert np.array_equal(b, par["binout"])
+
+
+@pytest.mark.parametrize("name", APPLY)
+@pytest.mark.parametrize("kidx", [0, 1])
+def test_operators_match_reference(name, kidx):
+    par = load_pre(name)
+    ap = load_apply(name)
+    N = par["N"]
+    k = par["kpoints"][kidx]
+    L = fo.lambdas(k, par)
+    assert L.Nd == int(ap[f"Nd_{kidx}"])
+    x = ap["x"]
+    x0 = x[: 2 * L.Nd]
+    v0 = x[2 * N: 5 * N]  # the harness reads v0 at double offset 4N (complex offset 2N)
+    B = edge_eps(par)
+    y = fo.Qr(x0, L)
+    ref = ap[f"Qr_{kidx}"]
+    assert np.linalg.norm(y - ref) <= 1e-12 * np.linalg.norm(ref)
+    y = fo.Qrs(v0, L)
+    ref = ap[f"Qrs_{kidx}"]
+    assert np.linalg.norm(y - ref) <= 1e-12 * np.linalg.norm(ref)
+    y = fo.QBQ(x0, L, 1.0 / B)
+    ref = ap[f"QBQ_{kidx}"]
+    assert np.linalg.norm(y - ref) <= 1e-12 * np.linalg.norm(ref)
+    y = fo.invAr(x0, L, 1.0 / B, 1e-10, 1000)
+    ref = ap[f"invAr_{kidx}"]
+    # both solves stop at ||r|| < 1e-10 in the CG variable (absolute); compare the
+    # solutions relative to their size with the CG tolerance as the bar
+    assert np.linalg.norm(y - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+def test_qrs_qr_identity():
+    par = load_pre("fcc16")
+    L = fo.lambdas(par["kpoints"][3], par)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(2 * L.Nd) + 1j * rng.standard_normal(2 * L.Nd)
+    assert np.linalg.norm(fo.Qrs(fo.Qr(x, L), L) - x) <= 1e-12 * np.linalg.norm(x)
+
+
+@pytest.mark.parametrize("name,kidx", [("sc16", 1), ("sc16", 0), ("bcc12", 2)])
+def test_solve_matches_reference_frequencies(name, kidx):
+    par = load_pre(name)
+    ref = load_ref(name)
+    rec = next(r for r in ref["kpoints"] if r["k"] == kidx)
+    B = edge_eps(par)
+    nwant = len(rec["freq"])
+    r = fo.solve_k(np.array(rec["wave_vec"]), par, B, dict(nwant=nwant, nstep=40, tol=1e-10, maxit=100),
+                   dict(tol=1e-10, maxit=1000))
+    assert r.Nd == rec["Nd"]
+    f = np.array(rec["freq"])
+    nz = f > 0
+    assert np.all(r.freq[~nz] == 0)
+    assert np.max(np.abs(r.freq[nz] - f[nz]) / f[nz]) < 1e-9
+    # same Lanczos path: identical A_r^-1 call count
+    assert r.es_iter == rec["es_iter"]
