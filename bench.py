@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Band-structure throughput benchmark (k-points/s) on B200.
+
+Workload: simple cubic lattice a=1, grid 96^3, one dielectric sphere (r=0.25a,
+eps=13) in eps=1, 10 bands, Lanczos restart dimension 40, Lanczos and CG
+tolerances 1e-10 (relative residual of every band checked <= 1e-6), the
+reference's default band path GXMGRX|MR with part_num=4 (20 k-points).  The k
+path and the material map are the reference preprocessing outputs committed in
+tests/golden/sc96_pre.npz (synthetic crystal; no dataset involved).
+
+One step = one full solve of the 20-k path through the device-resident solver
+(inputs already in HBM).  The working set of one batch is larger than L2 only in
+FP64; each step runs >1000 CG iterations, so L2 state between steps is irrelevant
+(config records "l2": "inputs exceed L2 per step").
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision mixed|fp64] [--no-fp64] [--no-cpu-baseline]
+
+--impl reference runs the reference's own FP64 CUDA build (oracle/_ref, compiled
+from the reference sources) through its own FAME_Fast_Algorithms_Driver on a
+bounded sample of the same path (4 k-points per step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fame-isotropic-gpu_b200"))
+
+METRIC = "k-points/s at 96^3, 10 bands, resid 1e-6: batched FP32 vs plain FP64, 1 B200"
+WORKLOAD = "sc96"
+NWANT, NSTEP = 10, 40
+TOLS = dict(es_tol=1e-10, ls_tol=1e-10, es_maxit=100, ls_maxit=1000)
+
+
+def load_workload():
+    z = np.load(os.path.join(ROOT, "tests", "golden", f"{WORKLOAD}_pre.npz"))
+    n = int(z["Binout_len"])
+    return dict(
+        grid=tuple(int(v) for v in z["grid_nums"]), mesh_len=z["mesh_len"], lattice_vec_a=z["lattice_vec_a"],
+        simple=bool(int(z["simple"][0])), m=tuple(int(v) for v in z["m"]), t1=z["t"][:3],
+        binout=np.unpackbits(z["Binout_bits"])[:n].astype(np.int32), material_num=int(z["material_num"][0]),
+        eps_in=z["ele_permitt_in"], eps_out=float(z["ele_permitt_out"][0]),
+        kpoints=z["WaveVector"].reshape(-1, 3))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 4 + i and
+                          s[4 + i].lower() in ("active", "1", "yes")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws == 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, ws, local, dist
+
+
+def max_over_ranks(x, dist):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def rank_kpoints(W, rank):
+    """Weak scaling: every rank solves a 20-point path; rank r's copy is shifted by
+    r*1e-3 (Cartesian, no 2*pi) so that ranks solve distinct k-points of equal cost."""
+    k = W["kpoints"].copy()
+    if rank:
+        k = k + 1e-3 * rank
+    return k
+
+
+def cpu_baseline(W, es_mean, counters):
+    """The oracle (numpy/scipy FP64 restatement of the reference method) timed on the
+    host cores: one A_r^-1 application (full CG to 1e-10) at a non-Gamma k of the
+    path, scaled by the mean A_r^-1 count per k-point of this run."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fame_oracle as fo
+    import scipy.fft as sfft
+    cores = os.cpu_count() or 1
+    par = dict(simple=W["simple"], grid=W["grid"], mesh_len=W["mesh_len"], lattice_vec_a=W["lattice_vec_a"],
+               m=W["m"], t1=W["t1"])
+    N = int(np.prod(W["grid"]))
+    B = fo.matrix_B(W["binout"], W["material_num"], W["eps_in"], W["eps_out"], N)
+    k = W["kpoints"][1]
+    L = fo.lambdas(k, par)
+    rng = np.random.default_rng(0)
+    u = rng.standard_normal(2 * L.Nd) + 1j * rng.standard_normal(2 * L.Nd)
+    u /= np.linalg.norm(u)
+    cnt = {"ls_iter": 0, "es_iter": 0}
+    with sfft.set_workers(cores):
+        # route the oracle's numpy FFT calls through scipy.fft's multithreaded backend
+        saved = (np.fft.fftn, np.fft.ifftn)
+        np.fft.fftn = lambda a, *x, **y: sfft.fftn(a, workers=cores)
+        np.fft.ifftn = lambda a, *x, **y: sfft.ifftn(a, workers=cores)
+        try:
+            t0 = time.perf_counter()
+            fo.invAr(u, L, 1.0 / B, TOLS["ls_tol"], TOLS["ls_maxit"], cnt)
+            t = time.perf_counter() - t0
+        finally:
+            np.fft.fftn, np.fft.ifftn = saved
+    per_k = t * es_mean
+    return {"value": 1.0 / per_k, "unit": "k-points/s", "cores": cores, "kind": "port",
+            "sample": f"oracle (numpy+scipy.fft FP64) A_r^-1 at 96^3 k={list(np.round(k, 4))}: "
+                      f"{cnt['ls_iter']} CG products in {t:.2f}s, x mean {es_mean:.1f} A_r^-1 per k "
+                      f"(Lanczos reorthogonalisation not included: lower bound on CPU time)"}
+
+
+def run_ours(args):
+    import torch
+    import fame_b200 as fb
+    rank, ws, local, dist = dist_init()
+    torch.cuda.set_device(local)
+    W = load_workload()
+    ctx = fb.Context(W["grid"], W["mesh_len"], W["lattice_vec_a"], W["simple"], W["m"], W["t1"], device=local)
+    ctx.set_material(W["binout"], W["material_num"], W["eps_in"], W["eps_out"])
+    N = int(np.prod(W["grid"]))
+    kp = rank_kpoints(W, rank)
+    nk = kp.shape[0]
+    prec = fb.MIXED if args.precision == "mixed" else fb.FP64
+    params = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=prec, batch=args.batch, **TOLS)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    out = None
+    for _ in range(args.warmup):
+        out = ctx.solve(kp, params)
+    barrier(dist)
+    torch.cuda.synchronize()
+    l0 = ctx.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            out = ctx.solve(kp, params)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(dist)
+    dt = ev0.elapsed_time(ev1) / 1e3
+    launches = ctx.launch_count() - l0
+    T = max_over_ranks(dt, dist)
+    value = nk * ws * args.steps / T
+    # ---- end to end through the public API: host eps -> device, solve, host results
+    B_host = edge_eps(W, N)
+    e2e_steps = max(1, min(args.steps, 2))
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.set_eps(B_host)
+        out_e2e = ctx.solve(kp, params)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e = {"value": nk * ws * e2e_steps / t_e2e, "unit": "k-points/s", "h2d_bytes_per_step": int(B_host.nbytes + kp.nbytes),
+           "d2h_bytes_per_step": int(3 * nk * NWANT * 8 + nk * 24), "steps": e2e_steps}
+    # ---- accuracy of this run
+    relres_max = float(np.max(out["relres"]))
+    fr = out["freq"]
+    ref_err = None
+    refp = os.path.join(ROOT, "tests", "golden", f"{WORKLOAD}_ref.json")
+    if rank == 0 and os.path.exists(refp):
+        ref = json.load(open(refp))
+        rf = np.array([r["freq"] for r in ref["kpoints"]])
+        nz = rf > 0
+        ref_err = float(np.max(np.abs(fr[nz] - rf[nz]) / rf[nz]))
+    counters = out["counters"]
+    es_mean = float(np.mean([c["es_iter"] for c in counters]))
+    ls_sum = int(sum(c["ls_iter"] for c in counters))
+    # ---- roofline of the dominant kernel: one Q_r^* B^-1 Q_r apply (3 fused stages)
+    hbm, src = peaks()
+    kq = kp[1]
+    ms, stages = ctx.bench_qbq(kq, prec, reps=20)
+    s = 8 if prec == fb.MIXED else 16
+    r = 4 if prec == fb.MIXED else 8
+    alg = (2 * 2 * N + 6 * N) * s + 3 * N * r  # B_QBQ = (2M + 6N)s + 3N r per apply
+    achieved = alg / (ms * 1e-3) / 1e9
+    stage_bytes = [(2 * N + 3 * N) * s, 6 * N * s + 3 * N * r, (3 * N + 2 * N) * s]
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "qbq_traffic.json")
+    if os.path.exists(tp):
+        tj = json.load(open(tp)).get("fp32" if prec == fb.MIXED else "fp64")
+        if tj and tj.get("grid") == list(W["grid"]):
+            traffic = tj.get("dram_bytes_per_apply")
+    roof = {"bound": "hbm", "kernel": "QBQ apply = plane_inv + pencil + plane_fwd",
+            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+            "peak_source": src, "traffic": traffic, "algorithmic_bytes": alg, "ms_per_apply": round(ms, 5),
+            "stage_ms": [round(x, 5) for x in stages],
+            "stage_GBps": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(stage_bytes, stages)],
+            "l2": "flushed (256 MiB write) before every apply"}
+    # ---- the plain FP64 form on the same path (the metric's comparison)
+    fp64 = None
+    if prec == fb.MIXED and not args.no_fp64:
+        p64 = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=fb.FP64, batch=args.batch, **TOLS)
+        o64 = ctx.solve(kp, p64)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        o64 = ctx.solve(kp, p64)
+        ev1.record(stream)
+        ev1.synchronize()
+        t64 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist)
+        nz = o64["freq"] > 0
+        fp64 = {"value": nk * ws / t64, "unit": "k-points/s", "speedup_mixed_over_fp64": round(value / (nk * ws / t64), 3),
+                "max_rel_freq_diff_mixed_vs_fp64": float(np.max(np.abs(fr[nz] - o64["freq"][nz]) / o64["freq"][nz])),
+                "max_relres_fp64": float(np.max(o64["relres"]))}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(W, es_mean, counters)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "k-points/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(T / args.steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 operator/CG + f64 refinement/Lanczos"
+            if prec == fb.MIXED else "f64", "data": "synthetic (reference preprocessing of a synthetic SC crystal)",
+            "config": {"workload": "SC a=1, 96^3, sphere r=0.25 eps=13 in eps=1, 10 bands, nstep 40, "
+                                   "tol 1e-10, path GXMGRX|MR part_num=4 (20 k-points per GPU)",
+                       "grid": list(W["grid"]), "kpoints_per_gpu": nk, "precision": args.precision,
+                       "batch": args.batch or "auto", "graph": True, "parallelism": f"k-sharding x{ws}",
+                       "l2": "inputs exceed L2 per step (>1000 CG iterations per step)"},
+            "accuracy": {"max_relres": relres_max, "max_rel_err_vs_reference_fp64": ref_err,
+                         "max_relerr_vs_fp64_rayleigh": float(np.max(out["relerr"]))},
+            "counters": {"es_iter_mean": es_mean, "ls_iter_total": ls_sum,
+                         "restarts_total": int(sum(c["restarts"] for c in counters))},
+            "roofline": roof, "plain_fp64": fp64, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def edge_eps(W, N):
+    """B (3N) from the material map with FAME_Matrix_B_Isotropic's last-wins rule."""
+    B = np.full(3 * N, W["eps_out"])
+    b = W["binout"].reshape(3, W["material_num"], N)
+    for c in range(3):
+        for j in range(W["material_num"]):
+            B[c * N:(c + 1) * N][b[c, j] == 1] = W["eps_in"][j]
+    return B
+
+
+def run_reference(args):
+    """The reference's own FP64 CUDA build (oracle/_ref/fame_ref_harness, compiled from
+    the reference sources by oracle/build_ref.sh) through its own preprocessing and
+    FAME_Fast_Algorithms_Driver; each step = 4 k-points of the same 20-k path."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    harness = os.path.join(ROOT, "oracle", "_ref", "fame_ref_harness")
+    if not os.path.exists(harness):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (oracle/build_ref.sh needs the reference sources)"}))
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_inputs as ri
+    per_step = 4
+    n = (args.warmup + args.steps) * per_step
+    kidx = ",".join(str(i % 20) for i in range(n))
+    with tempfile.TemporaryDirectory() as d:
+        ri.make_workdir(WORKLOAD, d)
+        out = os.path.join(d, "out.jsonl")
+        with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            rc = subprocess.run([harness, "solve", d, out, "--kidx", kidx], stdout=subprocess.DEVNULL,
+                                stderr=subprocess.PIPE, text=True)
+        if rc.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build failed rc={rc.returncode}: {rc.stderr[-200:]}"}))
+            return
+        recs = [json.loads(l) for l in open(out)]
+    timed = recs[args.warmup * per_step:]
+    t = sum(r["wall_s"] for r in timed)
+    value = len(timed) / t
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "k-points/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "SC a=1, 96^3, sphere r=0.25 eps=13 in eps=1, 10 bands, nstep 40, tol 1e-10, "
+                               "path GXMGRX|MR part_num=4", "grid": [96, 96, 96], "kpoints_per_step": per_step,
+                   "parallelism": "none (the reference runs one GPU, one k at a time)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "k-points/s", "cores": 1, "kind": "reference",
+                         "sample": f"{len(timed)} k-points of the 96^3 path through the reference's own FP64 "
+                                   "CUDA build (FAME_Fast_Algorithms_Driver; cuFFT/cuBLAS on the B200, one host "
+                                   "thread); the reference has no CPU implementation of this path"},
+        "e2e": {"value": round(value, 4), "unit": "k-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_counters": {"es_iter": [r["es_iter"] for r in timed], "ls_iter": [r["ls_iter"] for r in timed]},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -83,6 +83,13 @@ __device__ __forceinline__ float2 expipi(float x) {
   return make_float2(c, s);
 }
 
+// Kernels launched on the device, counted by each kernel's first thread.
+__device__ unsigned long long g_launches;
+#define FAME_COUNT_LAUNCH()                                                              \
+  do {                                                                                   \
+    if ((threadIdx.x | threadIdx.y | blockIdx.x | blockIdx.y | blockIdx.z) == 0) atomicAdd(&::fame::g_launches, 1ull); \
+  } while (0)
+
 // Status codes returned through the C ABI (include/fame_b200.h).
 enum Status : int {
   kOk = 0,

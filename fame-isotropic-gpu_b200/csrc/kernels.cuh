@@ -31,16 +31,40 @@ struct LzState {
   int pad;
 };
 
-// Condition output for CUDA-graph WHILE nodes; in host-driven mode only `flag`
-// is used.
+// Condition of one CUDA-graph WHILE node (in host-driven mode only `flag` is used).
+// Every loop is fail-safe: the first kernel of the body clears the condition, the
+// deciding kernel sets it again only while work remains and the loop's trip count
+// (counted on the device) is below `cap`; hitting the cap records an overflow in
+// trips[1] and ends the loop, so no data-dependent loop can run unbounded.
 struct Cond {
   cudaGraphConditionalHandle handle;
   int* flag;
+  int* trips;  // [0] trips of the current loop, [1] overflow marker
+  int cap;
 };
 
 __device__ __forceinline__ void set_cond(const Cond& c, int v) {
+  if (!c.flag) return;
   *c.flag = v;
   if (c.handle) cudaGraphSetConditional(c.handle, (unsigned)v);
+}
+
+// decision at the end of a loop body
+__device__ __forceinline__ void decide_cond(const Cond& c, int any) {
+  if (c.trips) {
+    const int t = ++c.trips[0];
+    if (any && t >= c.cap) {
+      c.trips[1] = 1;
+      any = 0;
+    }
+  }
+  set_cond(c, any);
+}
+
+// before the loop: reset the trip counter and set the first decision
+__device__ __forceinline__ void start_cond(const Cond& c, int any) {
+  if (c.trips) c.trips[0] = 0;
+  set_cond(c, any);
 }
 
 // Ticket counter over the whole grid: true in exactly one CTA, the last one.
@@ -63,6 +87,7 @@ __device__ __forceinline__ bool grid_last(unsigned* ctr, unsigned total) {
 // Per-k tables (FAME_Main/FAME_Matrix_Lambdas.cu:77-244 Simple, :288-489 General)
 // computed on the device: one thread per table entry, FP64 sincospi.
 __global__ void k_tables(Geom g, const Slot* slots, double2* tabs, double m1, double m2, double m3) {
+  FAME_COUNT_LAUNCH();
   const int slot = blockIdx.y;
   const Slot sl = slots[slot];
   double2* t = tabs + (size_t)slot * g.tab_stride;
@@ -144,12 +169,15 @@ struct PlaneInArgs {
   const float2* x32;      // IN_REFINE: FP32 correction
   int sigma;              // IN_VEC: multiply the input by sqrt(Lambda_q) first (Sigma, …_Isotropic.cu:109)
   cplx<R>* T;             // output field (3 components)
+  Cond reset;             // loop condition cleared by this kernel when it starts a loop body
 };
 
 // One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
 template <typename R, bool GEN, int IN, bool PR>
 __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512)
     k_plane_inv(PlaneInArgs<R> a) {
+  FAME_COUNT_LAUNCH();
+  if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(a.reset, 0);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* plane = reinterpret_cast<cplx<R>*>(smem_raw);
   const Geom& g = a.g;
@@ -287,6 +315,7 @@ struct PencilArgs {
 // grid = (Lm * ceil(Lf/TW), 3 * vec_per_slot, nslots)
 template <typename R, bool GEN, int MODE>
 __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
+  FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geom& g = a.g;
   const int TW = a.TW;
@@ -392,6 +421,7 @@ struct PlaneOutArgs {
 template <typename R, bool GEN, int EPI, bool PR>
 __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512)
     k_plane_fwd(PlaneOutArgs<R> a) {
+  FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* plane = reinterpret_cast<cplx<R>*>(smem_raw);
   const Geom& g = a.g;
@@ -412,7 +442,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512)
         if (threadIdx.x == 0) {
           int any = 0;
           for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && a.cg[q].outer_active;
-          set_cond(a.cond, any);
+          decide_cond(a.cond, any);
         }
       }
     }
@@ -513,7 +543,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512)
         if (threadIdx.x == 0) {
           int any = 0;
           for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && a.cg[q].outer_active;
-          set_cond(a.cond, any);
+          decide_cond(a.cond, any);
         }
       }
     }

@@ -91,9 +91,11 @@ __device__ __forceinline__ void pi_at(bool general, bool pr, double2 dLx, double
     p2[2] = cscale(cconj(t3), i2);
   } else {
     const cplx<R> Ls = cadd(cadd(Lx, Ly), Lz);
-    const R Lp = cabs2(Ls);
-    const R d1 = 3 * Lq * Lq - Lq * Lp, d2 = 3 * Lq - Lp;
-    const R i1 = (R)1 / sqrt(d1 > 0 ? d1 : (R)0), i2 = (R)1 / sqrt(d2 > 0 ? d2 : (R)0);
+    // 3*Lq - |Ls|^2 (the reference's normaliser, …Lambdas.cu:450-451) written as
+    // |Lx-Ly|^2 + |Ly-Lz|^2 + |Lz-Lx|^2: the same number without cancellation
+    const R d2 = cabs2(csub(Lx, Ly)) + cabs2(csub(Ly, Lz)) + cabs2(csub(Lz, Lx));
+    const R d1 = Lq * d2;
+    const R i1 = (R)1 / sqrt(d1), i2 = (R)1 / sqrt(d2);
     const cplx<R> cs = cconj(Ls);
     p1[0] = cscale(csub(mk<R>(Lq, 0), cmul(Lx, cs)), i1);
     p1[1] = cscale(csub(mk<R>(Lq, 0), cmul(Ly, cs)), i1);

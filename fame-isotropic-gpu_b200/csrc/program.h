@@ -74,9 +74,12 @@ class Program {
   }
 
   // Condition object for one WHILE loop; pass it to the kernels that set it.
-  Cond make_cond(int* dflag) {
+  // `trips` (2 device ints) and `cap` bound the loop on the device.
+  Cond make_cond(int* dflag, int* trips, int cap) {
     Cond c;
     c.flag = dflag;
+    c.trips = trips;
+    c.cap = cap;
     c.handle = 0;
     if (graph_) FAME_CK(cudaGraphConditionalHandleCreate(&c.handle, root_, 0, 0));
     return c;

@@ -174,8 +174,9 @@ struct Ops {
   template <typename R, int IN, bool PR>
   void plane_inv(const cplx<R>* in, cplx<R>* T, int nvec, long vstride, long fstride, int sigma,
                  cplx<R>* p = nullptr, const cplx<R>* r = nullptr, double2* y64 = nullptr,
-                 const float2* x32 = nullptr) {
+                 const float2* x32 = nullptr, Cond reset = Cond{}) {
     PlaneInArgs<R> a;
+    a.reset = reset;
     a.g = g();
     a.slots = c->slots.p;
     a.tabs = c->tabs.p;
@@ -237,7 +238,7 @@ struct Ops {
 
   template <typename R, int EPI, bool PR>
   void plane_fwd(const cplx<R>* T, cplx<R>* out, int nvec, long vstride, long fstride,
-                 const cplx<R>* p = nullptr, const cplx<R>* b = nullptr, Cond cond = Cond{0, nullptr},
+                 const cplx<R>* p = nullptr, const cplx<R>* b = nullptr, Cond cond = Cond{},
                  double tol2 = 0) {
     PlaneOutArgs<R> a;
     a.g = g();
@@ -455,6 +456,7 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
 __global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* EV, const double2* AV,
                                                     long vstride, int nwant, const double* theta,
                                                     int nstep, double* stats) {
+  FAME_COUNT_LAUNCH();
   const int band = blockIdx.y, slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   if (!sl.active) return;
@@ -482,6 +484,7 @@ __global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* E
 // (FAME_Fast_Algorithms_Isotropic.cu:119-121).
 __global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, double2* E, long fstride,
                                                           int nwant, long n3) {
+  FAME_COUNT_LAUNCH();
   const int band = blockIdx.x, slot = blockIdx.y;
   if (!slots[slot].active) return;
   double2* e = E + (long)(slot * nwant + band) * fstride;
@@ -502,6 +505,7 @@ __global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, dou
 // permittivity per voxel (B_x = B_y = B_z = eps) the voxel gradient sums its three
 // edges.  Bands with w = 0 (Gamma patch) get zero gradient.
 __global__ void __launch_bounds__(1024) k_adj_den(const double2* E, const double* B, long n3, double* den) {
+  FAME_COUNT_LAUNCH();
   const int band = blockIdx.x;
   const double2* e = E + (long)band * n3;
   double acc[1] = {0.0};
@@ -513,6 +517,7 @@ __global__ void __launch_bounds__(1024) k_adj_den(const double2* E, const double
 
 __global__ void __launch_bounds__(256) k_adj_grad(const double2* E, const double* w, const double* den, long N,
                                                   double* grad) {
+  FAME_COUNT_LAUNCH();
   const int band = blockIdx.y;
   const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= N) return;
@@ -536,6 +541,13 @@ static std::string cfg_key(const SolveCfg& s, bool graph) {
 
 // invAr (FAME_Main/FAME_Matrix_Vector_Production_Isotropic_invAr.cu:8-48) for the
 // Lanczos vector u_j of every live slot, leaving w in U[:, j+1]; then one Lanczos step.
+// device ints of the loop conditions: flag of loop i at flags[i], its trip counter
+// and overflow marker at flags[kTrips + 2i]
+constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopNone = 3, kLoopRestart = 4, kTrips = 32;
+static Cond loop_cond(Program& P, int* flags, int id, int cap) {
+  return P.make_cond(flags + id, flags + kTrips + 2 * id, cap);
+}
+
 static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base) {
   fame_ctx* c = o.c;
   Program& P = o.P;
@@ -545,28 +557,29 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
   const long F = 3L * g.N;
   const double tol2 = s.ls_tol * s.ls_tol;
   if (!s.mixed) {
-    Cond cc = P.make_cond(flag_base + 0);
+    Cond cc = loop_cond(P, flag_base, kLoopCG, s.ls_maxit + 2);
     P.launch(k_invar_pro<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), L, j, c->r64.p, c->x64.p,
              (double2*)nullptr, tol2, s.ls_maxit);
     P.while_loop(cc, [&] {
-      o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p);
+      o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr, cc);
       o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 1);
       o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
       P.launch(k_cg_update<double>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
                (const double2*)c->p64.p, (const double2*)c->Ap64.p);
     });
-    P.launch(k_invar_epi<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j,
+    P.launch(k_invar_epi<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j,
              (const double2*)c->x64.p);
   } else {
-    Cond outer = P.make_cond(flag_base + 1);
-    Cond inner = P.make_cond(flag_base + 2);
+    Cond outer = loop_cond(P, flag_base, kLoopOuter, 42);
+    Cond inner = loop_cond(P, flag_base, kLoopInner, s.inner_maxit + 2);
     P.launch(k_invar_pro<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(outer), L, j, c->r64.p, c->x64.p,
              c->b64.p, tol2, s.ls_maxit);
     P.while_loop(outer, [&] {
       P.launch(k_cg32_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), (const double2*)c->r64.p,
-               c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit);
+               c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit, outer);
       P.while_loop(inner, [&] {
-        o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p);
+        o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr,
+                                         inner);
         o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 1);
         o.plane_fwd<float, EPI_CG, false>(c->T32.p, c->Ap32.p, 1, M, F, c->p32.p);
         P.launch(k_cg_update<float>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), c->x32.p, c->r32.p,
@@ -577,12 +590,12 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
       o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 2);
       o.plane_fwd<double, EPI_RESID, false>(c->T64.p, c->r64.p, 1, M, F, nullptr, c->b64.p, outer, tol2);
     });
-    P.launch(k_invar_epi<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j,
+    P.launch(k_invar_epi<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j,
              (const double2*)c->x64.p);
   }
   const int ndots = (int)((M + kLzRows - 1) / kLzRows);
-  P.launch(k_lz_dots, dim3(ndots, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j);
-  P.launch(k_lz_update, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flag_base + 3}), L, j);
+  P.launch(k_lz_dots, dim3(ndots, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j);
+  P.launch(k_lz_update, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j);
 }
 
 static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
@@ -608,9 +621,9 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
   const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
   P.launch(k_tables, dim3((tmax + 255) / 256, s.nslots), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
            (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
-  P.launch(k_lz_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}), L);
+  P.launch(k_lz_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L);
   for (int j = 0; j < s.nstep; j++) emit_step(o, s, L, j, flags);
-  Cond restart = P.make_cond(flags + 4);
+  Cond restart = loop_cond(P, flags, kLoopRestart, s.es_maxit + 2);
   TriArgs ta;
   ta.L = L;
   ta.slots = c->slots.p;
@@ -623,26 +636,28 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
   ta.nslots = s.nslots;
   ta.status = c->status.p;
   ta.ctr = c->tri_ctr.p;
+  ta.first = 1;
   const size_t tsm = tridiag_smem(s.nstep);
   allow_smem(k_tridiag, tsm);
   P.launch(k_tridiag, dim3(s.nslots), dim3(32), tsm, ta);
+  ta.first = 0;
   P.while_loop(restart, [&] {
     for (int c0 = 0; c0 <= s.nwant; c0 += 8)
-      P.launch(k_ugemm<8>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}), L,
-               (const double*)c->G.p, s.nstep + 1, s.nstep + 1, s.nwant + 1, 0, (double2*)nullptr, c0);
+      P.launch(k_ugemm<8>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(restart), L, (const double*)c->G.p,
+               s.nstep + 1, s.nstep + 1, s.nwant + 1, 0, (double2*)nullptr, c0);
     P.launch(k_remap, dim3(s.nslots), dim3(32), 0, L, (const Slot*)c->slots.p, s.nslots);
     for (int j = s.nwant; j < s.nstep; j++) emit_step(o, s, L, j, flags);
     P.launch(k_tridiag, dim3(s.nslots), dim3(32), tsm, ta);
   });
   // Ritz vectors ev = U(:, 0:nstep) z(:, 0:nwant)   (Lanczos_Isotropic.cu:93)
   for (int c0 = 0; c0 < s.nwant; c0 += 8)
-    P.launch(k_ugemm<8>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}), L, (const double*)c->Z.p,
+    P.launch(k_ugemm<8>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, (const double*)c->Z.p,
              s.nstep, s.nstep, s.nwant, 1, c->EV.p, c0);
   // FP64 residual and Rayleigh quotient per band: v = QBQ(Sigma y)
   o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
   o.pencil<double, PEN_QBQ>(c->Tb.p, s.nwant, F, c->invB64.p, 0);
   o.plane_fwd<double, EPI_OUT, false>(c->Tb.p, c->AV.p, s.nwant, M, F);
-  P.launch(k_band_stats, dim3(1, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{0, flags + 3}),
+  P.launch(k_band_stats, dim3(1, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{}),
            (const double2*)c->EV.p, (const double2*)c->AV.p, M, s.nwant, (const double*)c->theta.p, s.nstep,
            c->stats.p);
   if (s.vec) {
@@ -827,7 +842,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     ensure_workspace(c, s.nslots, s.nstep, s.nwant, s.mixed, s.vec);
     const std::string key = cfg_key(s, graph);
     auto it = c->progs.find(key);
-    Program* P;
+    Program* P = nullptr;
     if (graph) {
       if (it == c->progs.end()) {
         auto prog = std::make_unique<Program>(c->stream, true, c->hflag, 0);
@@ -862,6 +877,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
       }
       FAME_CK(cudaMemcpyAsync(c->slots.p, hs.data(), s.nslots * sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
       FAME_CK(cudaMemsetAsync(c->status.p, 0, s.nslots * sizeof(int), c->stream));
+      FAME_CK(cudaMemsetAsync(c->flags.p, 0, 64 * sizeof(int), c->stream));
       if (graph) {
         P->run();
       } else {
@@ -876,7 +892,14 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
       FAME_CK(cudaMemcpyAsync(prof.data(), c->prof.p, prof.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
       FAME_CK(cudaMemcpyAsync(status.data(), c->status.p, status.size() * sizeof(int), cudaMemcpyDeviceToHost,
                               c->stream));
+      int hflags[64];
+      FAME_CK(cudaMemcpyAsync(hflags, c->flags.p, sizeof(hflags), cudaMemcpyDeviceToHost, c->stream));
       FAME_CK(cudaStreamSynchronize(c->stream));
+      for (int id = 0; id < 8; id++)
+        if (hflags[kTrips + 2 * id + 1]) {
+          set_err("a device loop reached its trip cap (loop " + std::to_string(id) + ")");
+          return FAME_ERR_WATCHDOG;
+        }
       for (int q = 0; q < nb; q++) {
         const int kk = b0 + q;
         const bool gamma = hs[q].Nd == N - 1;
@@ -1018,7 +1041,7 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
           L.h = c->hcoef.p;
           L.lz = c->lz.p;
           L.prof = c->prof.p;
-          P.launch(k_lz_init, dim3(1, 1, 1), dim3(256), 0, o.va(Cond{0, c->flags.p + 3}), L);
+          P.launch(k_lz_init, dim3(1, 1, 1), dim3(256), 0, o.va(Cond{}), L);
           FAME_CK(cudaMemcpyAsync(c->U.p, x, 2L * sl.Nd * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
           SolveCfg s;
           memset(&s, 0, sizeof(s));
@@ -1027,17 +1050,18 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
           s.ls_tol = prm->ls_tol;
           s.mixed = 0;
           const int nvb = vec_blocks(c, 1);
-          Cond cc = P.make_cond(c->flags.p);
+          Cond cc = loop_cond(P, c->flags.p, kLoopCG, s.ls_maxit + 2);
           P.launch(k_invar_pro<false>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), L, 0, c->r64.p, c->x64.p,
                    (double2*)nullptr, s.ls_tol * s.ls_tol, s.ls_maxit);
           P.while_loop(cc, [&] {
-            o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p);
+            o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr,
+                                              cc);
             o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 1);
             o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
             P.launch(k_cg_update<double>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
                      (const double2*)c->p64.p, (const double2*)c->Ap64.p);
           });
-          P.launch(k_invar_epi<false>, dim3(nvb, 1, 1), dim3(256), 0, o.va(Cond{0, c->flags.p + 3}), L, 0,
+          P.launch(k_invar_epi<false>, dim3(nvb, 1, 1), dim3(256), 0, o.va(Cond{}), L, 0,
                    (const double2*)c->x64.p);
           FAME_CK(cudaMemcpyAsync(y, c->U.p + M, 2L * sl.Nd * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
           break;
@@ -1077,6 +1101,99 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
   } catch (const std::exception& e) {
     set_err(e.what());
     return FAME_ERR_WATCHDOG;
+  }
+  return FAME_OK;
+}
+
+void* fame_ctx_stream(fame_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int fame_launch_count(fame_ctx* c, unsigned long long* out) {
+  if (!c || !out) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    FAME_CK(cudaStreamSynchronize(c->stream));
+    FAME_CK(cudaMemcpyFromSymbol(out, g_launches, sizeof(unsigned long long)));
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  return FAME_OK;
+}
+
+int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, double* ms_out, double* stage_ms) {
+  if (!c || !k || !ms_out || reps < 1 || (precision != FAME_FP64 && precision != FAME_MIXED)) {
+    set_err("bad argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (!c->have_eps) {
+    set_err("permittivity not set");
+    return FAME_ERR_BAD_INPUT;
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    ensure_workspace(c, 1, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), precision == FAME_MIXED,
+                     c->cap_vec);
+    Slot sl;
+    memset(&sl, 0, sizeof(sl));
+    thetas(c->lat, k, sl.th);
+    sl.Nd = reduced_size(c->lat, k);
+    sl.off = c->g.N - sl.Nd;
+    sl.active = 1;
+    FAME_CK(cudaMemcpyAsync(c->slots.p, &sl, sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
+    Program P(c->stream, false, c->hflag, 1);
+    Ops o{c, P, 1};
+    const Geom& g = c->g;
+    const long M = 2L * g.N, F = 3L * g.N;
+    const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
+    P.launch(k_tables, dim3((tmax + 255) / 256, 1), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
+             (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
+    DBuf<unsigned char> flush;
+    const size_t fl = 256ull << 20;
+    flush.ensure(fl);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) FAME_CK(cudaEventCreate(&e));
+    double tot[3] = {0, 0, 0};
+    // input: r64 / r32 hold arbitrary finite data after a memset
+    if (precision == FAME_FP64)
+      FAME_CK(cudaMemsetAsync(c->r64.p, 0, M * sizeof(double2), c->stream));
+    else
+      FAME_CK(cudaMemsetAsync(c->r32.p, 0, M * sizeof(float2), c->stream));
+    for (int it = 0; it < reps + 1; it++) {
+      FAME_CK(cudaMemsetAsync(flush.p, it & 0xff, fl, c->stream));
+      FAME_CK(cudaEventRecord(ev[0], c->stream));
+      if (precision == FAME_FP64) {
+        o.plane_inv<double, IN_VEC, false>(c->r64.p, c->T64.p, 1, M, F, 0);
+        FAME_CK(cudaEventRecord(ev[1], c->stream));
+        o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 0);
+        FAME_CK(cudaEventRecord(ev[2], c->stream));
+        o.plane_fwd<double, EPI_OUT, false>(c->T64.p, c->x64.p, 1, M, F);
+      } else {
+        o.plane_inv<float, IN_VEC, false>(c->r32.p, c->T32.p, 1, M, F, 0);
+        FAME_CK(cudaEventRecord(ev[1], c->stream));
+        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 0);
+        FAME_CK(cudaEventRecord(ev[2], c->stream));
+        o.plane_fwd<float, EPI_OUT, false>(c->T32.p, c->x32.p, 1, M, F);
+      }
+      FAME_CK(cudaEventRecord(ev[3], c->stream));
+      FAME_CK(cudaEventSynchronize(ev[3]));
+      if (it == 0) continue;  // warm-up
+      for (int q = 0; q < 3; q++) {
+        float ms = 0;
+        FAME_CK(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+        tot[q] += ms;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    flush.release();
+    *ms_out = (tot[0] + tot[1] + tot[2]) / reps;
+    if (stage_ms)
+      for (int q = 0; q < 3; q++) stage_ms[q] = tot[q] / reps;
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
   }
   return FAME_OK;
 }

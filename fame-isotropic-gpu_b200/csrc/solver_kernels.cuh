@@ -25,6 +25,7 @@ struct VecArgs {
 template <typename R>
 __global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* x, cplx<R>* r,
                                                    const cplx<R>* p, const cplx<R>* Ap) {
+  FAME_COUNT_LAUNCH();
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   CgState* st = va.cg + slot;
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* x, cplx<
     if (threadIdx.x == 0) {
       int any = 0;
       for (int q = 0; q < va.nslots; q++) any |= va.slots[q].active && va.cg[q].active;
-      set_cond(va.cond, any);
+      decide_cond(va.cond, any);
     }
   }
 }
@@ -95,6 +96,7 @@ __device__ __forceinline__ double2* ucol(const LzArgs& L, int slot, int logical)
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_invar_pro(VecArgs va, LzArgs L, int j, double2* r64,
                                                    double2* x64, double2* b64, double tol2, int maxit) {
+  FAME_COUNT_LAUNCH();
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   CgState* st = va.cg + slot;
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(256) k_invar_pro(VecArgs va, LzArgs L, int j, 
       int any = 0;
       for (int q = 0; q < va.nslots; q++)
         any |= va.slots[q].active && (MIXED ? va.cg[q].outer_active : va.cg[q].active);
-      set_cond(va.cond, any);
+      start_cond(va.cond, any);
     }
   }
 }
@@ -158,7 +160,9 @@ __global__ void __launch_bounds__(256) k_invar_pro(VecArgs va, LzArgs L, int j, 
 // Start of one FP32 inner solve: r32 = (float)(r64 * scale), x32 = 0; stop when
 // ||r32||^2 <= tau^2 ||r32_0||^2 or after `maxit` products.
 __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r64, float2* r32,
-                                                   float2* x32, double tau2, int maxit) {
+                                                   float2* x32, double tau2, int maxit, Cond outer_reset) {
+  FAME_COUNT_LAUNCH();
+  if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(outer_reset, 0);
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   CgState* st = va.cg + slot;
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r6
     if (threadIdx.x == 0) {
       int any = 0;
       for (int q = 0; q < va.nslots; q++) any |= va.slots[q].active && va.cg[q].active;
-      set_cond(va.cond, any);
+      start_cond(va.cond, any);
     }
   }
 }
@@ -207,6 +211,7 @@ __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r6
 // (…invAr.cu:41-43: ls_iter += k, es_iter++).
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, const double2* x64) {
+  FAME_COUNT_LAUNCH();
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   if (!sl.active || L.lz[slot].converged) return;
@@ -245,6 +250,7 @@ __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, 
 constexpr int kLzRows = 2048;  // rows per CTA, staged in shared memory (32 KB)
 
 __global__ void __launch_bounds__(256) k_lz_dots(VecArgs va, LzArgs L, int j) {
+  FAME_COUNT_LAUNCH();
   __shared__ double2 wsh[kLzRows];
   __shared__ double red[(2 * 64 + 1) * 8];  // [value][warp]
   const int slot = blockIdx.z;
@@ -325,6 +331,7 @@ __global__ void __launch_bounds__(256) k_lz_dots(VecArgs va, LzArgs L, int j) {
 
 // u_{j+1} = (w' - sum_i <u_i, w'> u_i) / beta_j
 __global__ void __launch_bounds__(256) k_lz_update(VecArgs va, LzArgs L, int j) {
+  FAME_COUNT_LAUNCH();
   __shared__ double2 hs[64];
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
@@ -359,6 +366,7 @@ __global__ void __launch_bounds__(256) k_lz_update(VecArgs va, LzArgs L, int j) 
 
 // e_M start vector (Lanczos_decomp_gpu.cu:93-107) and map/pool initialisation.
 __global__ void k_lz_init(VecArgs va, LzArgs L) {
+  FAME_COUNT_LAUNCH();
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   if (blockIdx.x == 0 && threadIdx.x <= L.nstep) L.map[slot * (L.nstep + 1) + threadIdx.x] = threadIdx.x;
@@ -402,6 +410,7 @@ struct TriArgs {
   int nslots;
   int* status;     // [nslots] 0 ok, 2 no convergence, 3 QL failure
   unsigned* ctr;   // grid ticket counter
+  int first;       // 1: the call before the restart loop (starts it), 0: end of a loop body
 };
 
 // dynamic shared memory of k_tridiag for nstep = n
@@ -430,6 +439,7 @@ __device__ void givens_ref(double a, double b, double& c, double& s, double& r) 
 }
 
 __global__ void __launch_bounds__(32) k_tridiag(TriArgs a) {
+  FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) double tsm[];
   const LzArgs& L = a.L;
   const int n = L.nstep, nw = L.nwant, lane = threadIdx.x;
@@ -658,7 +668,10 @@ __global__ void __launch_bounds__(32) k_tridiag(TriArgs a) {
     *a.ctr = 0u;
     int any = 0;
     for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && !a.L.lz[q].converged;
-    set_cond(a.cond, any);
+    if (a.first)
+      start_cond(a.cond, any);
+    else
+      decide_cond(a.cond, any);
   }
 }
 
@@ -671,6 +684,8 @@ __global__ void __launch_bounds__(32) k_tridiag(TriArgs a) {
 template <int CH>
 __global__ void __launch_bounds__(256) k_ugemm(VecArgs va, LzArgs L, const double* G, int ldg, int nrows,
                                                int ncols, int mode, double2* out, int c0) {
+  FAME_COUNT_LAUNCH();
+  if (mode == 0 && c0 == 0 && (threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(va.cond, 0);
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
   if (!sl.active) return;
@@ -720,6 +735,7 @@ __global__ void __launch_bounds__(256) k_ugemm(VecArgs va, LzArgs L, const doubl
 // After the restart product: logical 0..nwant -> the former free columns; the old
 // columns become the new pool (first nstep-nwant reused as logical nwant+1..nstep).
 __global__ void k_remap(LzArgs L, const Slot* slots, int nslots) {
+  FAME_COUNT_LAUNCH();
   const int slot = blockIdx.x;
   if (threadIdx.x != 0 || !slots[slot].active || L.lz[slot].converged) return;
   int* mp = L.map + slot * (L.nstep + 1);

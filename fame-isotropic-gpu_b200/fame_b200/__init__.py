@@ -1,0 +1,218 @@
+"""Python binding of the FAME B200 band-structure library (include/fame_b200.h).
+
+The compute path is the CUDA library libfame_b200.so built in-tree
+(fame-isotropic-gpu_b200/Makefile).  This module only marshals arguments through
+ctypes; there is no Python or CPU fallback: if the library or a CUDA device is
+missing, the calls raise.
+
+Mirrors the reference's interface for the path (paths relative to its project root):
+  - Context.solve      <- FAME_Fast_Algorithms_Driver over the k-loop of FAME_Main_Code
+                          (FAME_Main/FAME_Main_Code.cu:79-171)
+  - Context.apply      <- FAME_Matrix_Vector_Production_{Qr,Qrs,Pr,Prs,Isotropic_QBQ,
+                          Isotropic_invAr}
+  - Context.set_material <- FAME_Matrix_B_Isotropic (FAME_Main/FAME_Matrix_B_Isotropic.cu)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_HERE, "libfame_b200.so")
+
+OK, ERR_BAD_INPUT, ERR_NO_CONVERGENCE, ERR_WATCHDOG, ERR_CUDA, ERR_NO_DEVICE, ERR_UNSUPPORTED = range(7)
+FP64, MIXED = 0, 1
+OP_QR, OP_QRS, OP_QBQ, OP_PR, OP_PRS, OP_INVAR = range(6)
+
+# every symbol declared in include/fame_b200.h
+EXPORTS = ("fame_ctx_create", "fame_ctx_destroy", "fame_set_eps", "fame_set_material", "fame_solve_kpoints",
+           "fame_apply", "fame_adjoint", "fame_ctx_sizes", "fame_last_error", "fame_version", "fame_ctx_stream",
+           "fame_launch_count", "fame_bench_qbq")
+
+
+class FameError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fame error {code}: {msg}")
+        self.code = code
+
+
+class Lattice(C.Structure):
+    _fields_ = [("grid", C.c_int * 3), ("mesh_len", C.c_double * 3), ("lattice_vec_a", C.c_double * 9),
+                ("simple", C.c_int), ("m", C.c_int * 4), ("t1", C.c_double * 3)]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("nwant", C.c_int), ("nstep", C.c_int), ("es_maxit", C.c_int), ("es_tol", C.c_double),
+                ("ls_maxit", C.c_int), ("ls_tol", C.c_double), ("precision", C.c_int), ("batch", C.c_int),
+                ("use_graph", C.c_int), ("inner_tol", C.c_double), ("inner_maxit", C.c_int),
+                ("want_vectors", C.c_int)]
+
+
+class KCounters(C.Structure):
+    _fields_ = [("ls_iter", C.c_int), ("es_iter", C.c_int), ("restarts", C.c_int), ("status", C.c_int),
+                ("Nd", C.c_int), ("pad", C.c_int)]
+
+
+_lib = None
+
+
+def load():
+    """Loads libfame_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FameError(ERR_UNSUPPORTED, f"{LIB_PATH} not built (run __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.fame_ctx_create.argtypes = [C.c_int, C.POINTER(Lattice), C.POINTER(P)]
+    lib.fame_ctx_destroy.argtypes = [P]
+    lib.fame_ctx_destroy.restype = None
+    lib.fame_set_eps.argtypes = [P, D]
+    lib.fame_set_material.argtypes = [P, C.POINTER(C.c_int), C.c_int, D, C.c_double]
+    lib.fame_solve_kpoints.argtypes = [P, D, C.c_int, C.POINTER(SolverParams), D, D, D, D, C.POINTER(KCounters)]
+    lib.fame_apply.argtypes = [P, C.c_int, D, P, P, C.c_int, C.POINTER(SolverParams), C.POINTER(C.c_int)]
+    lib.fame_adjoint.argtypes = [P, D, D, C.c_int, C.c_int, D]
+    lib.fame_ctx_sizes.argtypes = [P, C.POINTER(C.c_longlong)]
+    lib.fame_ctx_stream.argtypes = [P]
+    lib.fame_ctx_stream.restype = C.c_void_p
+    lib.fame_launch_count.argtypes = [P, C.POINTER(C.c_ulonglong)]
+    lib.fame_bench_qbq.argtypes = [P, D, C.c_int, C.c_int, D, D]
+    lib.fame_last_error.restype = C.c_char_p
+    lib.fame_version.restype = C.c_char_p
+    for fn in ("fame_ctx_create", "fame_set_eps", "fame_set_material", "fame_solve_kpoints", "fame_apply",
+               "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq"):
+        getattr(lib, fn).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise FameError(rc, load().fame_last_error().decode())
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_lattice(grid, mesh_len, lattice_vec_a, simple, m=(0, 0, 0, 0), t1=(0.0, 0.0, 0.0)):
+    L = Lattice()
+    L.grid[:] = [int(v) for v in grid]
+    L.mesh_len[:] = [float(v) for v in mesh_len]
+    L.lattice_vec_a[:] = [float(v) for v in lattice_vec_a]
+    L.simple = int(bool(simple))
+    L.m[:] = [int(v) for v in m]
+    L.t1[:] = [float(v) for v in t1]
+    return L
+
+
+def solver_params(nwant=10, nstep=40, es_maxit=100, es_tol=1e-10, ls_maxit=1000, ls_tol=1e-10,
+                  precision=FP64, batch=0, use_graph=1, inner_tol=0.0, inner_maxit=0, want_vectors=0):
+    p = SolverParams()
+    p.nwant, p.nstep, p.es_maxit, p.es_tol = nwant, nstep, es_maxit, es_tol
+    p.ls_maxit, p.ls_tol, p.precision, p.batch = ls_maxit, ls_tol, precision, batch
+    p.use_graph, p.inner_tol, p.inner_maxit, p.want_vectors = use_graph, inner_tol, inner_maxit, want_vectors
+    return p
+
+
+class Context:
+    """One device, one grid/lattice, one permittivity field."""
+
+    def __init__(self, grid, mesh_len, lattice_vec_a, simple, m=(0, 0, 0, 0), t1=(0.0, 0.0, 0.0), device=0):
+        lib = load()
+        self._lat = make_lattice(grid, mesh_len, lattice_vec_a, simple, m, t1)
+        self.N = int(np.prod(grid))
+        h = C.c_void_p()
+        _check(lib.fame_ctx_create(device, C.byref(self._lat), C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_par(cls, par, device=0):
+        return cls(par["grid"], par["mesh_len"], par["lattice_vec_a"], par["simple"], par["m"], par["t1"], device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fame_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_eps(self, B):
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        assert B.size == 3 * self.N
+        _check(load().fame_set_eps(self._h, _dptr(B)))
+
+    def set_material(self, binout, material_num, eps_in, eps_out):
+        b = np.ascontiguousarray(binout, dtype=np.int32)
+        e = np.ascontiguousarray(eps_in, dtype=np.float64)
+        _check(load().fame_set_material(self._h, b.ctypes.data_as(C.POINTER(C.c_int)), int(material_num),
+                                        _dptr(e), float(eps_out)))
+
+    def solve(self, kpoints, params=None, **kw):
+        """Returns dict(freq, relres, relerr, counters[, evec]) for kpoints (nk, 3)."""
+        p = params or solver_params(**kw)
+        k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        nk = k.shape[0]
+        freq = np.zeros((nk, p.nwant))
+        rr = np.zeros((nk, p.nwant))
+        re = np.zeros((nk, p.nwant))
+        ev = np.zeros((nk, p.nwant, 3 * self.N), dtype=np.complex128) if p.want_vectors else None
+        cnt = (KCounters * nk)()
+        rc = load().fame_solve_kpoints(self._h, _dptr(k), nk, C.byref(p), _dptr(freq), _dptr(rr), _dptr(re),
+                                       ev.ctypes.data_as(C.POINTER(C.c_double)) if ev is not None else None, cnt)
+        out = dict(freq=freq, relres=rr, relerr=re, rc=rc,
+                   counters=[dict(ls_iter=c.ls_iter, es_iter=c.es_iter, restarts=c.restarts, status=c.status,
+                                  Nd=c.Nd) for c in cnt])
+        if ev is not None:
+            out["evec"] = ev
+        if rc not in (OK, ERR_NO_CONVERGENCE):
+            _check(rc)
+        return out
+
+    def apply(self, op, k, x, y, precision=FP64, params=None):
+        """Applies operator `op` at wave vector k to device buffers x -> y (torch CUDA
+        tensors, complex128 for FP64 / complex64 for MIXED).  Returns Nd."""
+        kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+        nd = C.c_int()
+        p = params or solver_params()
+        _check(load().fame_apply(self._h, int(op), _dptr(kk), C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                 int(precision), C.byref(p), C.byref(nd)))
+        return nd.value
+
+    def stream(self):
+        """The context's cudaStream_t as an int (for torch.cuda.ExternalStream)."""
+        return load().fame_ctx_stream(self._h)
+
+    def launch_count(self):
+        n = C.c_ulonglong()
+        _check(load().fame_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def bench_qbq(self, k, precision=MIXED, reps=20):
+        """Mean device ms of one L2-cold Q_r^* B^-1 Q_r apply and of its 3 stages."""
+        kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+        ms = C.c_double()
+        st = np.zeros(3)
+        _check(load().fame_bench_qbq(self._h, _dptr(kk), int(precision), int(reps), C.byref(ms), _dptr(st)))
+        return ms.value, st
+
+    def adjoint(self, freq, evec):
+        """d(omega_i)/d(eps_voxel) for one k: freq (nwant,), evec (nwant, 3N) complex128 host."""
+        f = np.ascontiguousarray(freq, dtype=np.float64)
+        e = np.ascontiguousarray(evec, dtype=np.complex128)
+        nw = f.size
+        g = np.zeros((nw, self.N))
+        _check(load().fame_adjoint(self._h, _dptr(f), e.ctypes.data_as(C.POINTER(C.c_double)), nw, 1, _dptr(g)))
+        return g
+
+
+def version():
+    return load().fame_version().decode()

@@ -130,6 +130,23 @@ int fame_apply(fame_ctx* ctx, int op, const double* k_xyz, const void* in, void*
 int fame_adjoint(fame_ctx* ctx, const double* freq, const double* evec, int nwant, int host,
                  double* grad_out);
 
+/* The context's CUDA stream (a cudaStream_t), so callers can time work on it with
+ * CUDA events.  All device work of the context runs on this stream. */
+void* fame_ctx_stream(fame_ctx* ctx);
+
+/* Number of kernels of this library launched on the device so far (counted on the
+ * device by every kernel's first thread, graph-launched kernels included). */
+int fame_launch_count(fame_ctx* ctx, unsigned long long* count_out);
+
+/* Operator benchmark: `reps` applications of Q_r^* B^-1 Q_r at wave vector k in
+ * FP64 (precision FAME_FP64) or FP32 (FAME_MIXED), each preceded by an L2 flush
+ * (a 256 MiB device write) outside the timed span; CUDA events on the context
+ * stream.  stage_ms_out[3] (optional) receives the mean device time of the plane
+ * inverse stage, the pencil stage and the plane forward stage; ms_out the mean of
+ * their sum. */
+int fame_bench_qbq(fame_ctx* ctx, const double* k, int precision, int reps, double* ms_out,
+                   double* stage_ms_out);
+
 /* Grid size N and maximum reduced size 2N of the context, for buffer sizing. */
 int fame_ctx_sizes(const fame_ctx* ctx, long long* N_out);
 
