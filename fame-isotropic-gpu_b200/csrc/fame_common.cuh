@@ -83,8 +83,15 @@ __device__ __forceinline__ float2 expipi(float x) {
   return make_float2(c, s);
 }
 
-// Kernels launched on the device, counted by each kernel's first thread.
-__device__ unsigned long long g_launches;
+// Kernels launched on the device, counted by each kernel's first thread.  Every
+// translation unit has its own counter; FAME_DEFINE_LAUNCH_GETTER exposes it.
+static __device__ unsigned long long g_launches;
+#define FAME_DEFINE_LAUNCH_GETTER(fn)                                              \
+  unsigned long long fn() {                                                        \
+    unsigned long long v = 0;                                                      \
+    if (cudaMemcpyFromSymbol(&v, ::fame::g_launches, sizeof(v)) != cudaSuccess) v = 0; \
+    return v;                                                                      \
+  }
 #define FAME_COUNT_LAUNCH()                                                              \
   do {                                                                                   \
     if ((threadIdx.x | threadIdx.y | blockIdx.x | blockIdx.y | blockIdx.z) == 0) atomicAdd(&::fame::g_launches, 1ull); \

@@ -30,27 +30,41 @@ struct AxisPlan {
   int radix[kMaxPasses];
 };
 
-// cos/sin(2*pi*m/R) for the odd radices handled by the symmetric-pair DFT,
-// filled once from the host (fame_fft_init_constants) with libm in FP64.
-__constant__ double c_cos7[7], c_sin7[7], c_cos11[11], c_sin11[11], c_cos13[13], c_sin13[13];
-__constant__ double c_cos5[5], c_sin5[5];
-
+// cos/sin(2*pi*m/R) for the odd radices handled by the symmetric-pair DFT
+// (mathematical constants, correctly rounded to double).  m is a compile-time
+// constant at every use, so each call folds to a literal.
 template <int RAD> struct OddTab;
 template <> struct OddTab<5> {
-  __device__ static double c(int m) { return c_cos5[m]; }
-  __device__ static double s(int m) { return c_sin5[m]; }
+  __device__ __forceinline__ static constexpr double c(int m) {
+    return m == 0 ? 1.0 : m == 1 ? 0.30901699437494745 : m == 2 ? -0.8090169943749475 : m == 3 ? -0.8090169943749475 : 0.30901699437494745;
+  }
+  __device__ __forceinline__ static constexpr double s(int m) {
+    return m == 0 ? 0.0 : m == 1 ? 0.9510565162951535 : m == 2 ? 0.5877852522924731 : m == 3 ? -0.5877852522924731 : -0.9510565162951535;
+  }
 };
 template <> struct OddTab<7> {
-  __device__ static double c(int m) { return c_cos7[m]; }
-  __device__ static double s(int m) { return c_sin7[m]; }
+  __device__ __forceinline__ static constexpr double c(int m) {
+    return m == 0 ? 1.0 : m == 1 ? 0.6234898018587335 : m == 2 ? -0.2225209339563144 : m == 3 ? -0.9009688679024191 : m == 4 ? -0.9009688679024191 : m == 5 ? -0.2225209339563144 : 0.6234898018587335;
+  }
+  __device__ __forceinline__ static constexpr double s(int m) {
+    return m == 0 ? 0.0 : m == 1 ? 0.7818314824680298 : m == 2 ? 0.9749279121818236 : m == 3 ? 0.4338837391175581 : m == 4 ? -0.4338837391175581 : m == 5 ? -0.9749279121818236 : -0.7818314824680298;
+  }
 };
 template <> struct OddTab<11> {
-  __device__ static double c(int m) { return c_cos11[m]; }
-  __device__ static double s(int m) { return c_sin11[m]; }
+  __device__ __forceinline__ static constexpr double c(int m) {
+    return m == 0 ? 1.0 : m == 1 ? 0.8412535328311812 : m == 2 ? 0.41541501300188644 : m == 3 ? -0.14231483827328514 : m == 4 ? -0.6548607339452851 : m == 5 ? -0.9594929736144974 : m == 6 ? -0.9594929736144974 : m == 7 ? -0.6548607339452851 : m == 8 ? -0.14231483827328514 : m == 9 ? 0.41541501300188644 : 0.8412535328311812;
+  }
+  __device__ __forceinline__ static constexpr double s(int m) {
+    return m == 0 ? 0.0 : m == 1 ? 0.5406408174555976 : m == 2 ? 0.9096319953545183 : m == 3 ? 0.9898214418809327 : m == 4 ? 0.7557495743542583 : m == 5 ? 0.28173255684142967 : m == 6 ? -0.28173255684142967 : m == 7 ? -0.7557495743542583 : m == 8 ? -0.9898214418809327 : m == 9 ? -0.9096319953545183 : -0.5406408174555976;
+  }
 };
 template <> struct OddTab<13> {
-  __device__ static double c(int m) { return c_cos13[m]; }
-  __device__ static double s(int m) { return c_sin13[m]; }
+  __device__ __forceinline__ static constexpr double c(int m) {
+    return m == 0 ? 1.0 : m == 1 ? 0.8854560256532099 : m == 2 ? 0.5680647467311558 : m == 3 ? 0.12053668025532305 : m == 4 ? -0.3546048870425356 : m == 5 ? -0.7485107481711011 : m == 6 ? -0.970941817426052 : m == 7 ? -0.970941817426052 : m == 8 ? -0.7485107481711011 : m == 9 ? -0.3546048870425356 : m == 10 ? 0.12053668025532305 : m == 11 ? 0.5680647467311558 : 0.8854560256532099;
+  }
+  __device__ __forceinline__ static constexpr double s(int m) {
+    return m == 0 ? 0.0 : m == 1 ? 0.46472317204376856 : m == 2 ? 0.8229838658936564 : m == 3 ? 0.992708874098054 : m == 4 ? 0.9350162426854148 : m == 5 ? 0.6631226582407952 : m == 6 ? 0.23931566428755777 : m == 7 ? -0.23931566428755777 : m == 8 ? -0.6631226582407952 : m == 9 ? -0.9350162426854148 : m == 10 ? -0.992708874098054 : m == 11 ? -0.8229838658936564 : -0.46472317204376856;
+  }
 };
 
 // multiply by -i (forward) or +i (inverse)
@@ -141,8 +155,8 @@ template <typename R, int RAD> struct DftOdd {
       Q[s - 1] = csub(a[s], a[RAD - s]);
       sum = cadd(sum, P[s - 1]);
     }
-    cplx<R> out[RAD];
-    out[0] = sum;
+    // a[1..RAD-1] are free now (kept in P, Q): write the outputs in place
+    a[0] = sum;
 #pragma unroll
     for (int t = 1; t <= H; t++) {
       cplx<R> re = x0, im = mk<R>(0, 0);
@@ -156,11 +170,9 @@ template <typename R, int RAD> struct DftOdd {
         im.y += sn * Q[s - 1].y;
       }
       cplx<R> r = rot_mi(im, inv);  // -i*im (forward) / +i*im (inverse)
-      out[t] = cadd(re, r);
-      out[RAD - t] = csub(re, r);
+      a[t] = cadd(re, r);
+      a[RAD - t] = csub(re, r);
     }
-#pragma unroll
-    for (int t = 0; t < RAD; t++) a[t] = out[t];
   }
 };
 template <typename R> struct Dft<R, 5> : DftOdd<R, 5> {};
@@ -168,140 +180,267 @@ template <typename R> struct Dft<R, 7> : DftOdd<R, 7> {};
 template <typename R> struct Dft<R, 11> : DftOdd<R, 11> {};
 template <typename R> struct Dft<R, 13> : DftOdd<R, 13> {};
 
-// Lines layout: element m of line l at buf[l*ls + m*es].  `line_fast` chooses the
-// thread->butterfly mapping so that consecutive threads touch consecutive shared
-// memory words: lines fastest when the lines are adjacent words (es > 1, ls = 1),
-// butterflies fastest when the line itself is contiguous (es = 1).
+// Lines layout: element m of line l at buf[l*ls + m*es].  Threads are mapped
+// lines-fastest: thread t works on line t mod nl, so consecutive threads touch
+// words ls apart.  Lines along the contiguous axis therefore use an odd padded
+// line stride (the plane row pitch), which makes every pass free of shared memory
+// bank conflicts for any radix; lines across the contiguous axis have ls = 1.
 struct LineSet {
   int nl, ls, es;
-  bool line_fast;
 };
 
-// One radix-RAD pass over lines [l0, l0 + nlg).
+// Exact unsigned division by an invariant divisor d for n * d < 2^32:
+// floor(n / d) = umulhi(n, ceil(2^32 / d)).
+struct Div {
+  unsigned m, d;
+  __device__ __forceinline__ explicit Div(unsigned dd) : m(0xffffffffu / dd + 1u), d(dd) {}
+  __device__ __forceinline__ unsigned q(unsigned n) const { return d == 1 ? n : __umulhi(n, m); }
+};
+
+// One radix-RAD Stockham pass over all lines, in place.  Every round stages the
+// butterflies of G complete lines in registers (read all, barrier, write all,
+// barrier): a line's outputs overwrite positions other butterflies of the same
+// line still read, so a line never spans two rounds.  Thread t works on line
+// l0 + t mod G and butterflies j = t / G + jstep * q (q < MAXB), with jstep * MAXB
+// >= n / RAD; consecutive threads touch consecutive lines.
 template <typename R, int RAD, int MAXB>
-__device__ __noinline__ void stockham_pass(cplx<R>* buf, int n, int Ns, LineSet L, int l0, int nlg,
-                                              const cplx<R>* tw, bool inv) {
-  const int nb_line = n / RAD;
-  const int total = nb_line * nlg;
+__device__ __forceinline__ void stockham_pass(cplx<R>* buf, int n, int Ns, LineSet L, const cplx<R>* tw,
+                                              bool inv) {
+  const int T = blockDim.x;
+  const int nb = n / RAD;
   const int stw = n / (Ns * RAD);
-  cplx<R> v[MAXB][RAD];
-  int dst[MAXB];
+  const int per_line = (nb + MAXB - 1) / MAXB;  // threads one line needs
+  const int G = min(L.nl, max(1, T / per_line));
+  const Div dg(G), dns(Ns);
+  const int t = threadIdx.x;
+  const int j0 = (int)dg.q(t);
+  const int lt = t - j0 * G;
+  const int jstep = T / G;
+  for (int l0 = 0; l0 < L.nl; l0 += G) {
+    const int l = l0 + lt;
+    const bool live = j0 < jstep && l < L.nl;
+    cplx<R>* base = buf + l * L.ls;
+    cplx<R> v[MAXB][RAD];
+    int dst[MAXB];
 #pragma unroll
-  for (int q = 0; q < MAXB; q++) {
-    const int b = threadIdx.x + q * blockDim.x;
-    dst[q] = -1;
-    if (b < total) {
-      int l, j;
-      if (L.line_fast) {
-        l = b % nlg;
-        j = b / nlg;
-      } else {
-        j = b % nb_line;
-        l = b / nb_line;
-      }
-      l += l0;
-      const int k = j % Ns;
-      const cplx<R>* src = buf + l * L.ls;
+    for (int q = 0; q < MAXB; q++) {
+      const int j = j0 + jstep * q;
+      dst[q] = -1;
+      if (live && j < nb) {
+        const int jb = (int)dns.q(j);
+        const int k = j - jb * Ns;
 #pragma unroll
-      for (int t = 0; t < RAD; t++) {
-        cplx<R> a = src[(j + t * nb_line) * L.es];
-        if (t > 0 && k > 0) {
-          cplx<R> w = tw[t * k * stw];
-          if (inv) w.y = -w.y;
-          a = cmul(a, w);
+        for (int u = 0; u < RAD; u++) {
+          cplx<R> a = base[(j + u * nb) * L.es];
+          if (u > 0 && k > 0) {
+            cplx<R> w = tw[u * k * stw];
+            if (inv) w.y = -w.y;
+            a = cmul(a, w);
+          }
+          v[q][u] = a;
         }
-        v[q][t] = a;
+        Dft<R, RAD>::run(v[q], inv);
+        dst[q] = (jb * Ns * RAD + k) * L.es;
       }
-      Dft<R, RAD>::run(v[q], inv);
-      dst[q] = l * L.ls + ((j / Ns) * Ns * RAD + k) * L.es;
     }
-  }
-  __syncthreads();
+    __syncthreads();
 #pragma unroll
-  for (int q = 0; q < MAXB; q++) {
-    if (dst[q] >= 0) {
+    for (int q = 0; q < MAXB; q++) {
+      if (dst[q] >= 0) {
 #pragma unroll
-      for (int t = 0; t < RAD; t++) buf[dst[q] + t * Ns * L.es] = v[q][t];
+        for (int u = 0; u < RAD; u++) base[dst[q] + u * Ns * L.es] = v[q][u];
+      }
     }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
-// Output-stationary DFT pass for an arbitrary radix r (used for large primes).
+// Output-stationary DFT pass for an arbitrary radix r (used for large primes):
+// rounds of G complete lines, thread t owns line l0 + t mod G and outputs
+// o = t / G + ostep * q.
 template <typename R, int MAXE>
-__device__ __noinline__ void generic_pass(cplx<R>* buf, int n, int r, int Ns, LineSet L, int l0, int nlg,
-                                             const cplx<R>* tw, bool inv) {
-  const int total = n * nlg;
+__device__ __forceinline__ void generic_pass(cplx<R>* buf, int n, int r, int Ns, LineSet L, const cplx<R>* tw,
+                                             bool inv) {
+  const int T = blockDim.x;
   const int stw = n / (Ns * r);
   const int nr = n / r;
-  cplx<R> v[MAXE];
-  int dst[MAXE];
+  const int per_line = (n + MAXE - 1) / MAXE;
+  const int G = min(L.nl, max(1, T / per_line));
+  const int t = threadIdx.x;
+  const int o0 = t / G;
+  const int lt = t - o0 * G;
+  const int ostep = T / G;
+  for (int l0 = 0; l0 < L.nl; l0 += G) {
+    const int l = l0 + lt;
+    const bool live = o0 < ostep && l < L.nl;
+    cplx<R>* base = buf + l * L.ls;
+    cplx<R> v[MAXE];
+    int dst[MAXE];
 #pragma unroll
-  for (int q = 0; q < MAXE; q++) {
-    const int b = threadIdx.x + q * blockDim.x;
-    dst[q] = -1;
-    if (b < total) {
-      int l, o;
-      if (L.line_fast) {
-        l = b % nlg;
-        o = b / nlg;
-      } else {
-        o = b % n;
-        l = b / n;
+    for (int q = 0; q < MAXE; q++) {
+      const int o = o0 + ostep * q;
+      dst[q] = -1;
+      if (live && o < n) {
+        const int k = o % Ns;
+        const int u = (o / Ns) % r;
+        const int j = (o / (Ns * r)) * Ns + k;
+        const int step = (k * stw + u * nr) % n;
+        int idx = 0;
+        const cplx<R>* src = base + j * L.es;
+        cplx<R> acc = mk<R>(0, 0);
+        for (int s = 0; s < r; s++) {
+          cplx<R> w = tw[idx];
+          if (inv) w.y = -w.y;
+          acc = cadd(acc, cmul(src[s * nr * L.es], w));
+          idx += step;
+          if (idx >= n) idx -= n;
+        }
+        v[q] = acc;
+        dst[q] = o * L.es;
       }
-      l += l0;
-      const int k = o % Ns;
-      const int t = (o / Ns) % r;
-      const int j = (o / (Ns * r)) * Ns + k;
-      const int step = (k * stw + t * nr) % n;
-      int idx = 0;
-      const cplx<R>* src = buf + l * L.ls + j * L.es;
-      cplx<R> acc = mk<R>(0, 0);
-      for (int s = 0; s < r; s++) {
-        cplx<R> w = tw[idx];
-        if (inv) w.y = -w.y;
-        acc = cadd(acc, cmul(src[s * nr * L.es], w));
-        idx += step;
-        if (idx >= n) idx -= n;
-      }
-      v[q] = acc;
-      dst[q] = l * L.ls + o * L.es;
     }
-  }
-  __syncthreads();
+    __syncthreads();
 #pragma unroll
-  for (int q = 0; q < MAXE; q++)
-    if (dst[q] >= 0) buf[dst[q]] = v[q];
-  __syncthreads();
+    for (int q = 0; q < MAXE; q++)
+      if (dst[q] >= 0) base[dst[q]] = v[q];
+    __syncthreads();
+  }
 }
 
-// Full transform of all lines along one axis.  Lines are independent, so each
-// pass is run over groups of lines small enough that a thread holds at most
-// about EMAX elements in registers; every group costs one barrier pair.
-template <typename R, int EMAX>
+// Full transform of all lines along one axis.  RARE selects whether the passes
+// for radix 7, 11, 13 and large primes are compiled in: they are register hungry,
+// so kernels for grids whose lengths factor into 2, 3, 4, 5, 8 leave them out
+// (the host picks the instantiation from the axis plans).  EMAX bounds the
+// elements a thread stages in registers per round.
+template <typename R, int EMAX, bool RARE>
 __device__ __forceinline__ void fft_lines(cplx<R>* buf, const AxisPlan P, LineSet L, const cplx<R>* tw,
-                                       bool inv) {
+                                          bool inv) {
   const int n = P.n;
-  const int per_group = max(1, (EMAX * (int)blockDim.x) / n);  // lines per group
+  constexpr int MB5 = EMAX / 5 > 2 ? 2 : (EMAX / 5 > 0 ? EMAX / 5 : 1);
   int Ns = 1;
   for (int p = 0; p < P.npass; p++) {
     const int r = P.radix[p];
-    for (int l0 = 0; l0 < L.nl; l0 += per_group) {
-      const int nlg = min(per_group, L.nl - l0);
-      switch (r) {
-        case 2: stockham_pass<R, 2, (EMAX + 1) / 2>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 3: stockham_pass<R, 3, (EMAX + 2) / 3>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 4: stockham_pass<R, 4, (EMAX + 3) / 4>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 5: stockham_pass<R, 5, (EMAX + 4) / 5>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 7: stockham_pass<R, 7, (EMAX + 6) / 7>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 8: stockham_pass<R, 8, (EMAX + 7) / 8>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 11: stockham_pass<R, 11, (EMAX + 10) / 11>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        case 13: stockham_pass<R, 13, (EMAX + 12) / 13>(buf, n, Ns, L, l0, nlg, tw, inv); break;
-        default: generic_pass<R, EMAX>(buf, n, r, Ns, L, l0, nlg, tw, inv); break;
-      }
+    switch (r) {
+      case 2: stockham_pass<R, 2, EMAX / 2>(buf, n, Ns, L, tw, inv); break;
+      case 3: stockham_pass<R, 3, EMAX / 3>(buf, n, Ns, L, tw, inv); break;
+      case 4: stockham_pass<R, 4, EMAX / 4>(buf, n, Ns, L, tw, inv); break;
+      case 5: stockham_pass<R, 5, MB5>(buf, n, Ns, L, tw, inv); break;
+      case 8: stockham_pass<R, 8, EMAX / 8>(buf, n, Ns, L, tw, inv); break;
+      default:
+        if constexpr (RARE) {
+          switch (r) {
+            case 7: stockham_pass<R, 7, (EMAX / 7 > 0 ? EMAX / 7 : 1)>(buf, n, Ns, L, tw, inv); break;
+            case 11: stockham_pass<R, 11, 1>(buf, n, Ns, L, tw, inv); break;
+            case 13: stockham_pass<R, 13, 1>(buf, n, Ns, L, tw, inv); break;
+            default: generic_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv); break;
+          }
+        }
+        break;
     }
     Ns *= r;
   }
+}
+
+
+// ---------------------------------------------------------------- compile-time plans
+// Static factorisation of a line length into the inlined radices 8, 4, 2, 5, 3
+// (same order as the host's runtime plans).
+constexpr int splan_count(int n) {
+  int c = 0;
+  const int rs[5] = {8, 4, 2, 5, 3};
+  for (int i = 0; i < 5; i++)
+    while (n % rs[i] == 0) {
+      n /= rs[i];
+      c++;
+    }
+  return n == 1 ? c : -1;
+}
+constexpr int splan_radix(int n, int p) {
+  const int rs[5] = {8, 4, 2, 5, 3};
+  int c = 0;
+  for (int i = 0; i < 5; i++)
+    while (n % rs[i] == 0) {
+      if (c == p) return rs[i];
+      n /= rs[i];
+      c++;
+    }
+  return 0;
+}
+
+// One radix-RAD pass with the line length N, line count NL and thread count T
+// compile-time: line stride ls, element stride es (constants fold when the caller
+// passes literals).  Same round structure as stockham_pass.
+template <typename R, int N, int NL, int T, int NS, int RAD, int MAXB>
+__device__ __forceinline__ void spass(cplx<R>* buf, int ls, int es, const cplx<R>* tw, bool inv) {
+  constexpr int nb = N / RAD;
+  constexpr int stw = N / (NS * RAD);
+  constexpr int per_line = (nb + MAXB - 1) / MAXB;
+  constexpr int G0 = T / per_line;
+  constexpr int G = G0 < 1 ? 1 : (G0 > NL ? NL : G0);
+  constexpr int jstep = T / G;
+  constexpr int rounds = (NL + G - 1) / G;
+  const int t = threadIdx.x;
+  const int j0 = t / G;
+  const int lt = t - j0 * G;
+#pragma unroll 1
+  for (int rd = 0; rd < rounds; rd++) {
+    const int l = rd * G + lt;
+    const bool live = j0 < jstep && (rounds * G == NL || l < NL);
+    cplx<R>* base = buf + l * ls;
+    cplx<R> v[MAXB][RAD];
+    bool on[MAXB];
+    int jbk[MAXB];
+#pragma unroll
+    for (int q = 0; q < MAXB; q++) {
+      const int j = j0 + jstep * q;
+      on[q] = live && (jstep * MAXB == nb || j < nb);
+      if (on[q]) {
+        const int jb = j / NS;  // compile-time divisor
+        const int k = j - jb * NS;
+        jbk[q] = jb * NS * RAD + k;
+#pragma unroll
+        for (int u = 0; u < RAD; u++) {
+          cplx<R> a = base[(j + u * nb) * es];
+          if (NS > 1 && u > 0) {
+            cplx<R> w = tw[u * k * stw];
+            if (inv) w.y = -w.y;
+            a = cmul(a, w);
+          }
+          v[q][u] = a;
+        }
+        Dft<R, RAD>::run(v[q], inv);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < MAXB; q++) {
+      if (on[q]) {
+#pragma unroll
+        for (int u = 0; u < RAD; u++) base[(jbk[q] + u * NS) * es] = v[q][u];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename R, int N, int NL, int T, int EMAX, int P = 0, int NS = 1>
+__device__ __forceinline__ void sfft(cplx<R>* buf, int ls, int es, const cplx<R>* tw, bool inv) {
+  static_assert(splan_count(N) > 0, "line length must factor into 2, 3, 4, 5, 8");
+  if constexpr (P < splan_count(N)) {
+    constexpr int RAD = splan_radix(N, P);
+    constexpr int MB = RAD == 5 ? (EMAX / 5 > 2 ? 2 : (EMAX / 5 > 0 ? EMAX / 5 : 1)) : (EMAX / RAD > 0 ? EMAX / RAD : 1);
+    spass<R, N, NL, T, NS, RAD, MB>(buf, ls, es, tw, inv);
+    sfft<R, N, NL, T, EMAX, P + 1, NS * RAD>(buf, ls, es, tw, inv);
+  }
+}
+
+// true when every radix of the plan has an inlined pass in fft_lines<.., false>
+inline bool plan_is_common(const AxisPlan& P) {
+  for (int p = 0; p < P.npass; p++) {
+    const int r = P.radix[p];
+    if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) return false;
+  }
+  return true;
 }
 
 }  // namespace fame

@@ -1,0 +1,63 @@
+// Geometry policies of the operator kernels.
+//
+// DynGeom takes every length from the runtime Geom and runs the runtime-planned
+// FFT passes (any grid).  StatGeom<LF, LM, LS> fixes the fast, mid and slow line
+// lengths at compile time: the FFT passes are fully unrolled and all index
+// arithmetic folds to constants.  The solver instantiates StatGeom for the grids
+// it runs most (cubic 96^3) and falls back to DynGeom elsewhere.
+#pragma once
+#include "state.cuh"
+
+namespace fame {
+
+constexpr int kPlaneThreads = 512;   // threads of a plane CTA with a static geometry
+constexpr int kPencilThreads = 256;  // threads of a pencil CTA
+
+struct DynGeom {
+  static constexpr bool kStatic = false;
+  __device__ __forceinline__ static int Lf(const Geom& g) { return g.Lf; }
+  __device__ __forceinline__ static int Lm(const Geom& g) { return g.Lm; }
+  __device__ __forceinline__ static int Ls(const Geom& g) { return g.Ls; }
+  __device__ __forceinline__ static int S(const Geom& g) { return g.S; }
+  __device__ __forceinline__ static int P(const Geom& g) { return g.P; }
+  // lines of a plane (pitch S) along its fast axis (fast = true) or mid axis, and
+  // the TW lines of a pencil tile.  One FFT call site per kernel keeps the kernel
+  // within its register budget, so the plane axis is a runtime argument.
+  template <typename R, bool RARE>
+  __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom& g, bool fast, const cplx<R>* tw,
+                                                   bool inv) {
+    fft_lines<R, Emax<R>::v, RARE>(b, fast ? g.pf : g.pm, fast ? LineSet{g.Lm, g.S, 1} : LineSet{g.Lf, 1, g.S},
+                                   tw, inv);
+  }
+  template <typename R, bool RARE>
+  __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom& g, const cplx<R>* tw, bool inv) {
+    constexpr int TW = PencilTW<R>::v;
+    fft_lines<R, Emax<R>::v, RARE>(b, g.ps, LineSet{TW, 1, TW}, tw, inv);
+  }
+};
+
+template <int LF, int LM, int LSL>
+struct StatGeom {
+  static constexpr bool kStatic = true;
+  static constexpr int kS = LF | 1;
+  __device__ __forceinline__ static constexpr int Lf(const Geom&) { return LF; }
+  __device__ __forceinline__ static constexpr int Lm(const Geom&) { return LM; }
+  __device__ __forceinline__ static constexpr int Ls(const Geom&) { return LSL; }
+  __device__ __forceinline__ static constexpr int S(const Geom&) { return kS; }
+  __device__ __forceinline__ static constexpr int P(const Geom&) { return LF * LM; }
+  static_assert(LF == LM, "a static plane geometry has equal fast and mid lengths");
+  template <typename R, bool RARE>
+  __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom&, bool fast, const cplx<R>* tw,
+                                                   bool inv) {
+    sfft<R, LF, LM, kPlaneThreads, Emax<R>::v>(b, fast ? kS : 1, fast ? 1 : kS, tw, inv);
+  }
+  template <typename R, bool RARE>
+  __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom&, const cplx<R>* tw, bool inv) {
+    constexpr int TW = PencilTW<R>::v;
+    sfft<R, LSL, TW, kPencilThreads, Emax<R>::v>(b, 1, TW, tw, inv);
+  }
+};
+
+using Stat96 = StatGeom<96, 96, 96>;
+
+}  // namespace fame

@@ -1,0 +1,395 @@
+// Operator stage kernels (plane inverse, pencil, plane forward); explicitly
+// instantiated per precision, lattice family and geometry policy in ops_*.cu.
+//
+// GP is the geometry policy (geom_policy.cuh): runtime lengths (DynGeom) or
+// compile-time lengths (StatGeom<...>).
+#pragma once
+#include "geom_policy.cuh"
+
+namespace fame {
+
+// Lambda_x, Lambda_y, Lambda_z at plane element (m, f) of plane s, in precision R.
+// Simple lattices read the per-CTA shared tables lx[f], ly[m] and the plane's lz.
+template <typename R, bool GEN>
+__device__ __forceinline__ void lam_elem(const Geom& g, const double2* tab, const cplx<R>* lx, const cplx<R>* ly,
+                                         cplx<R> lz, int s, int m, int f, cplx<R>& Lx, cplx<R>& Ly,
+                                         cplx<R>& Lz) {
+  if constexpr (!GEN) {
+    Lx = lx[f];
+    Ly = ly[m];
+    Lz = lz;
+  } else {
+    double2 a, b, c;
+    lambdas_at(g, tab, s, m, f, a, b, c);
+    Lx = cvt<R>(a);
+    Ly = cvt<R>(b);
+    Lz = cvt<R>(c);
+  }
+}
+
+// One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
+template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
+    k_plane_inv(PlaneInArgs<R> a) {
+  FAME_COUNT_LAUNCH();
+  if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(a.reset, 0);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geom& g = a.g;
+  const int Lf = GP::Lf(g), Lm = GP::Lm(g), S = GP::S(g), P = GP::P(g);
+  cplx<R>* plane = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* twf = plane + Lm * S;  // plane rows have the odd pitch S >= Lf
+  cplx<R>* twm = twf + Lf;
+  cplx<R>* lx = twm + Lm;
+  cplx<R>* ly = lx + Lf;
+  cg::cluster_group cl = cg::this_cluster();
+  const int comp = (int)cl.block_rank();
+  const int s = blockIdx.x / 3;
+  const int vec = blockIdx.y;
+  const int slot = blockIdx.z;
+  const Slot sl = a.slots[slot];
+  if (!sl.active) return;  // uniform over the cluster
+  CgState* st = nullptr;
+  if constexpr (IN == IN_CG || IN == IN_REFINE) {
+    st = a.cg + slot;
+    if constexpr (IN == IN_CG) {
+      if (!st->active) return;
+    } else {
+      if (!st->outer_active) return;
+    }
+  }
+  const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
+  for (int i = threadIdx.x; i < Lf; i += blockDim.x) {
+    twf[i] = a.tw[g.twf + i];
+    if constexpr (!GEN) lx[i] = cvt<R>(tab[g.oLx + i]);
+  }
+  for (int i = threadIdx.x; i < Lm; i += blockDim.x) {
+    twm[i] = a.tw[g.twm + i];
+    if constexpr (!GEN) ly[i] = cvt<R>(tab[g.oLy + i]);
+  }
+  const cplx<R> lz = GEN ? mk<R>(0, 0) : cvt<R>(tab[g.oLz + s]);
+  cl.sync();  // every CTA of the cluster is running (and the tables are in place)
+
+  const long vb = (long)(slot * a.vec_per_slot + vec) * a.vstride;
+  const int Nd = sl.Nd, off = sl.off;
+  cplx<R>* dst[3] = {cl.map_shared_rank(plane, 0), cl.map_shared_rank(plane, 1),
+                     cl.map_shared_rank(plane, 2)};
+  const int per = (P + 2) / 3;
+  const int e0 = comp * per, e1 = min(P, e0 + per);
+  R beta = 0;
+  bool first = false;
+  R rscale = 0;
+  if constexpr (IN == IN_CG) {
+    first = st->iter == 1;
+    beta = (R)st->beta;
+  }
+  if constexpr (IN == IN_REFINE) rscale = (R)(1.0 / st->scale);
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int fi = s * P + e;
+    const int m = e / Lf, f = e - m * Lf;
+    cplx<R> v[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
+    if (fi >= off) {
+      const long i = fi - off;
+      cplx<R> Lx, Ly, Lz;
+      lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
+      cplx<R> x1, x2;
+      if constexpr (IN == IN_VEC) {
+        x1 = a.in[vb + i];
+        x2 = a.in[vb + Nd + i];
+        if (a.sigma) {
+          const R sc = sqrt(cabs2(Lx) + cabs2(Ly) + cabs2(Lz));
+          x1 = cscale(x1, sc);
+          x2 = cscale(x2, sc);
+        }
+      } else if constexpr (IN == IN_CG) {
+        const cplx<R> r1 = a.r[vb + i], r2 = a.r[vb + Nd + i];
+        if (first) {
+          x1 = r1;
+          x2 = r2;
+        } else {
+          const cplx<R> p1 = a.p[vb + i], p2 = a.p[vb + Nd + i];
+          x1 = mk<R>(r1.x + beta * p1.x, r1.y + beta * p1.y);
+          x2 = mk<R>(r2.x + beta * p2.x, r2.y + beta * p2.y);
+        }
+        a.p[vb + i] = x1;
+        a.p[vb + Nd + i] = x2;
+      } else {  // IN_REFINE (R = double): y += x32 / scale, mix y
+        const float2 c1 = a.x32[vb + i], c2 = a.x32[vb + Nd + i];
+        double2 y1 = a.y64[vb + i], y2 = a.y64[vb + Nd + i];
+        y1.x += (double)c1.x * rscale;
+        y1.y += (double)c1.y * rscale;
+        y2.x += (double)c2.x * rscale;
+        y2.y += (double)c2.y * rscale;
+        a.y64[vb + i] = y1;
+        a.y64[vb + Nd + i] = y2;
+        x1 = cvt<R>(y1);
+        x2 = cvt<R>(y2);
+      }
+      cplx<R> Pc[6];
+      pi_from<R>(GEN, PR, Lx, Ly, Lz, Pc);
+#pragma unroll
+      for (int c = 0; c < 3; c++) v[c] = cadd(cmul(Pc[c], x1), cmul(Pc[3 + c], x2));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) dst[c][m * S + f] = v[c];
+  }
+  cl.sync();
+
+  // inverse 2-D transform of this component's plane (unnormalised): fast axis,
+  // then mid axis.  One FFT call site per axis loop keeps the kernel within its
+  // register budget.
+  for (int ax = 0; ax < 2; ax++) {
+    GP::template fft_plane<R, RARE>(plane, g, ax == 0, ax == 0 ? twf : twm, true);
+    if constexpr (GEN) {
+      // x D_kz(x,y,z) after the z (fast) pass (FAME_FFT_CUDA.cu:278, kernel :452-487),
+      // x D_ky(x,y) after the y (mid) pass (FAME_FFT_CUDA.cu:284, kernel :367-404)
+      for (int e = threadIdx.x; e < P; e += blockDim.x) {
+        const int m = e / Lf, f = e - m * Lf;
+        const int q = m * S + f;
+        plane[q] = cmul(plane[q], ax == 0 ? dkz_at<R>(g, tab, s, m, f) : cvt<R>(tab[g.oDky + s * g.Ny + m]));
+      }
+      __syncthreads();
+    }
+  }
+  cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
+  for (int e = threadIdx.x; e < P; e += blockDim.x) {
+    const int m = e / Lf;
+    T[e] = plane[e + m * (S - Lf)];
+  }
+}
+
+// ------------------------------------------------------------------ pencil stage
+
+// grid = (Lm * ceil(Lf/TW), 3 * vec_per_slot, nslots), kPencilThreads threads
+template <typename R, bool GEN, int MODE, bool RARE, class GP>
+__global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
+  FAME_COUNT_LAUNCH();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geom& g = a.g;
+  constexpr int TW = PencilTW<R>::v;
+  const int Lf = GP::Lf(g), Ls = GP::Ls(g), P = GP::P(g);
+  cplx<R>* tile = reinterpret_cast<cplx<R>*>(smem_raw);  // [Ls][TW]
+  cplx<R>* tws = tile + Ls * TW;
+  const int slot = blockIdx.z;
+  const Slot sl = a.slots[slot];
+  if (!sl.active) return;
+  if (a.gate == 1 && !a.cg[slot].active) return;
+  if (a.gate == 2 && !a.cg[slot].outer_active) return;
+  const int comp = blockIdx.y % 3, vec = blockIdx.y / 3;
+  const int nft = (Lf + TW - 1) / TW;
+  const int m = blockIdx.x / nft;
+  const int f0 = (blockIdx.x - m * nft) * TW;
+  const int tw_n = min(TW, Lf - f0);
+  const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
+  for (int i = threadIdx.x; i < Ls; i += blockDim.x) tws[i] = a.tw[g.tws + i];
+  const long fb = (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N;
+  // ---- load
+  for (int q = threadIdx.x; q < Ls * TW; q += blockDim.x) {
+    const int s = q / TW, f = q - s * TW;
+    cplx<R> v = mk<R>(0, 0);
+    if (f < tw_n) {
+      if constexpr (MODE == PEN_QRS_IN) {
+        // spatial input, x conj(D) before the forward transform
+        long sp;
+        cplx<R> d;
+        if (!GEN) {
+          sp = (long)s * P + m * Lf + f0 + f;
+          const double2 dd = cmul(cmul(tab[g.oDz + s], tab[g.oDy + m]), tab[g.oDx + f0 + f]);
+          d = cvt<R>(cconj(dd));
+        } else {
+          sp = ((long)(f0 + f) * g.Ny + m) * g.Nx + s;
+          d = cvt<R>(cconj(tab[g.oDkx + s]));
+        }
+        v = cmul(a.in[(long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + sp], d);
+      } else {
+        v = a.T[fb + (long)s * P + m * Lf + f0 + f];
+      }
+    }
+    tile[q] = v;
+  }
+  __syncthreads();
+  // QBQ: inverse, x B^{-1}/N, forward.  QR_OUT: inverse, x D/N (and B^{-1}), store.
+  // QRS_IN: forward only.  One FFT call site (dir loop) for the register budget.
+  constexpr int ndir = MODE == PEN_QBQ ? 2 : 1;
+  for (int dir = 0; dir < ndir; dir++) {
+    const bool inv = MODE == PEN_QRS_IN ? false : dir == 0;
+    GP::template fft_slow<R, RARE>(tile, g, tws, inv);
+    if (MODE != PEN_QRS_IN && dir == 0) {
+      const R invN = (R)(1.0 / g.N);
+      for (int q = threadIdx.x; q < Ls * TW; q += blockDim.x) {
+        const int s = q / TW, f = q - s * TW;
+        if (f < tw_n) {
+          long sp;
+          if (!GEN)
+            sp = (long)s * P + m * Lf + f0 + f;
+          else
+            sp = ((long)(f0 + f) * g.Ny + m) * g.Nx + s;
+          if constexpr (MODE == PEN_QBQ) {
+            tile[q] = cscale(tile[q], a.invB[(long)comp * g.N + sp] * invN);
+          } else {
+            cplx<R> d;
+            if (!GEN)
+              d = cvt<R>(cmul(cmul(tab[g.oDz + s], tab[g.oDy + m]), tab[g.oDx + f0 + f]));
+            else
+              d = cvt<R>(tab[g.oDkx + s]);
+            cplx<R> v = cscale(cmul(tile[q], d), invN);
+            if (a.invB) v = cscale(v, a.invB[(long)comp * g.N + sp]);
+            a.out[(long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + sp] = v;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if constexpr (MODE == PEN_QBQ || MODE == PEN_QRS_IN) {
+    for (int q = threadIdx.x; q < Ls * TW; q += blockDim.x) {
+      const int s = q / TW, f = q - s * TW;
+      if (f < tw_n) a.T[fb + (long)s * P + m * Lf + f0 + f] = tile[q];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ plane stage (forward)
+
+template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
+    k_plane_fwd(PlaneOutArgs<R> a) {
+  FAME_COUNT_LAUNCH();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geom& g = a.g;
+  const int Lf = GP::Lf(g), Lm = GP::Lm(g), S = GP::S(g), P = GP::P(g);
+  cplx<R>* plane = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* twf = plane + Lm * S;  // plane rows have the odd pitch S >= Lf
+  cplx<R>* twm = twf + Lf;
+  cplx<R>* lx = twm + Lm;
+  cplx<R>* ly = lx + Lf;
+  cg::cluster_group cl = cg::this_cluster();
+  const int comp = (int)cl.block_rank();
+  const int s = blockIdx.x / 3;
+  const int vec = blockIdx.y;
+  const int slot = blockIdx.z;
+  const Slot sl = a.slots[slot];
+  bool live = sl.active;
+  if constexpr (EPI == EPI_CG) live = live && a.cg[slot].active;
+  if constexpr (EPI == EPI_RESID) live = live && a.cg[slot].outer_active;
+  if (!live) {
+    if constexpr (EPI == EPI_RESID) {
+      if (grid_last(a.counters + a.nslots, gridDim.x * gridDim.y * gridDim.z)) {
+        if (threadIdx.x == 0) {
+          int any = 0;
+          for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && a.cg[q].outer_active;
+          decide_cond(a.cond, any);
+        }
+      }
+    }
+    return;
+  }
+  const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
+  for (int i = threadIdx.x; i < Lf; i += blockDim.x) {
+    twf[i] = a.tw[g.twf + i];
+    if constexpr (!GEN) lx[i] = cvt<R>(tab[g.oLx + i]);
+  }
+  for (int i = threadIdx.x; i < Lm; i += blockDim.x) {
+    twm[i] = a.tw[g.twm + i];
+    if constexpr (!GEN) ly[i] = cvt<R>(tab[g.oLy + i]);
+  }
+  const cplx<R> lz = GEN ? mk<R>(0, 0) : cvt<R>(tab[g.oLz + s]);
+  const cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
+  for (int e = threadIdx.x; e < P; e += blockDim.x) {
+    const int m = e / Lf;
+    plane[e + m * (S - Lf)] = T[e];
+  }
+  __syncthreads();
+  // forward 2-D transform.  General lattices (T*, FAME_FFT_CUDA.cu:297-319):
+  // x conj(D_ky), y (mid) pass, x conj(D_kz), z (fast) pass.  Simple lattices:
+  // fast then mid axis, no twiddles.
+  for (int ax = 0; ax < 2; ax++) {
+    const bool fast = GEN ? ax == 1 : ax == 0;
+    if constexpr (GEN) {
+      for (int e = threadIdx.x; e < P; e += blockDim.x) {
+        const int m = e / Lf, f = e - m * Lf;
+        const int q = m * S + f;
+        plane[q] = cmul(plane[q], ax == 0 ? cvt<R>(cconj(tab[g.oDky + s * g.Ny + m]))
+                                          : cconj(dkz_at<R>(g, tab, s, m, f)));
+      }
+      __syncthreads();
+    }
+    GP::template fft_plane<R, RARE>(plane, g, fast, fast ? twf : twm, false);
+  }
+  cl.sync();  // all three component planes transformed
+
+  const cplx<R>* src[3] = {cl.map_shared_rank(plane, 0), cl.map_shared_rank(plane, 1),
+                           cl.map_shared_rank(plane, 2)};
+  const int per = (P + 2) / 3;
+  const int e0 = comp * per, e1 = min(P, e0 + per);
+  const int Nd = sl.Nd, off = sl.off;
+  const long vb = (long)(slot * a.vec_per_slot + vec) * a.vstride;
+  double acc[2] = {0.0, 0.0};
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int fi = s * P + e;
+    if (fi < off) continue;
+    const long i = fi - off;
+    const int m = e / Lf, f = e - m * Lf;
+    const int q = m * S + f;
+    const cplx<R> t0 = src[0][q], t1 = src[1][q], t2 = src[2][q];
+    cplx<R> Lx, Ly, Lz;
+    lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
+    cplx<R> Pc[6];
+    pi_from<R>(GEN, PR, Lx, Ly, Lz, Pc);
+    const cplx<R> o1 = cadd(cadd(cmulc(Pc[0], t0), cmulc(Pc[1], t1)), cmulc(Pc[2], t2));
+    const cplx<R> o2 = cadd(cadd(cmulc(Pc[3], t0), cmulc(Pc[4], t1)), cmulc(Pc[5], t2));
+    if constexpr (EPI == EPI_OUT) {
+      a.out[vb + i] = o1;
+      a.out[vb + Nd + i] = o2;
+    } else if constexpr (EPI == EPI_CG) {
+      a.out[vb + i] = o1;
+      a.out[vb + Nd + i] = o2;
+      const cplx<R> p1 = a.p[vb + i], p2 = a.p[vb + Nd + i];
+      const cplx<R> d = cadd(cmulc(p1, o1), cmulc(p2, o2));  // conj(p) Ap
+      acc[0] += (double)d.x;
+      acc[1] += (double)d.y;
+    } else {  // EPI_RESID
+      const cplx<R> r1 = csub(a.b[vb + i], o1), r2 = csub(a.b[vb + Nd + i], o2);
+      a.out[vb + i] = r1;
+      a.out[vb + Nd + i] = r2;
+      acc[0] += (double)(cabs2(r1) + cabs2(r2));
+    }
+  }
+  cl.sync();  // remote shared memory must outlive the readers
+
+  if constexpr (EPI == EPI_CG || EPI == EPI_RESID) {
+    __shared__ double sred[2 * 32];
+    block_reduce<2>(acc, sred);
+    const int nblk = gridDim.x;  // CTAs of this slot (vec_per_slot == 1 in solves)
+    double tot[2];
+    if (slot_reduce<2>(acc, a.partials + (size_t)slot * nblk * 2, a.counters + slot, blockIdx.x, nblk,
+                       tot)) {
+      if (threadIdx.x == 0) {
+        CgState* st = a.cg + slot;
+        if constexpr (EPI == EPI_CG) {
+          // a = r1 / dot  (CG.cu:325-328)
+          const double den = tot[0] * tot[0] + tot[1] * tot[1];
+          st->a_re = st->r1 * tot[0] / den;
+          st->a_im = -st->r1 * tot[1] / den;
+        } else {
+          st->rr = tot[0];
+          st->outer++;
+          st->outer_total++;
+          st->outer_active = (tot[0] > a.tol2) && (st->outer < st->outer_max);
+          st->scale = 1.0 / sqrt(tot[0] > 0 ? tot[0] : 1.0);
+        }
+        __threadfence();
+      }
+    }
+    if constexpr (EPI == EPI_RESID) {
+      if (grid_last(a.counters + a.nslots, gridDim.x * gridDim.y * gridDim.z)) {
+        if (threadIdx.x == 0) {
+          int any = 0;
+          for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && a.cg[q].outer_active;
+          decide_cond(a.cond, any);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace fame

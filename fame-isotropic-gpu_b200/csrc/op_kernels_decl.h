@@ -1,0 +1,24 @@
+// Declarations of the operator stage kernels; the definitions are in
+// op_kernels.cuh and instantiated in ops_*.cu.
+#pragma once
+#include "geom_policy.cuh"
+
+namespace fame {
+// shared memory of a plane CTA: plane [Lm x S] | twf [Lf] | twm [Lm] | lx [Lf] | ly [Lm]
+template <typename R>
+__host__ __device__ inline size_t plane_smem_bytes(int Lf, int Lm, int S) {
+  return sizeof(cplx<R>) * ((size_t)Lm * S + 2 * (size_t)Lf + 2 * (size_t)Lm);
+}
+
+template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP> __global__ void k_plane_inv(PlaneInArgs<R> a);
+template <typename R, bool GEN, int MODE, bool RARE, class GP> __global__ void k_pencil(PencilArgs<R> a);
+template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP> __global__ void k_plane_fwd(PlaneOutArgs<R> a);
+
+// combinations instantiated with a static geometry (the CG / refinement hot path
+// and the operator benchmark)
+template <typename R, int IN, bool PR>
+constexpr bool kStatInv = !PR && (IN == IN_CG || IN == IN_VEC || (IN == IN_REFINE && sizeof(R) == 8));
+template <typename R, int MODE> constexpr bool kStatPen = MODE == PEN_QBQ;
+template <typename R, int EPI, bool PR>
+constexpr bool kStatFwd = !PR && (EPI == EPI_CG || EPI == EPI_OUT || (EPI == EPI_RESID && sizeof(R) == 8));
+}  // namespace fame

@@ -35,6 +35,7 @@ struct Geom {
   int Nx, Ny, Nz, N;
   int general;
   int Ls, Lm, Lf, P;  // slow / mid / fast lengths, plane size
+  int S;              // row pitch of a plane in shared memory: Lf rounded up to odd
   double hx, hy, hz;
   AxisPlan pf, pm, ps;
   // per-slot table offsets (in double2 units) inside a slot's table block
@@ -69,10 +70,9 @@ __device__ __forceinline__ void lambdas_at(const Geom& g, const double2* tab, in
 
 // Pi_Qr columns (FAME_Main/FAME_Matrix_Lambdas.cu:184-244 Simple, :438-489 General),
 // or Pi_Pr = [-conj(Pi2); conj(Pi1)] when pr is set.  P[0..2] multiply x1, P[3..5] x2.
+// Lambdas in the operator precision R; the normalisers use rsqrt.
 template <typename R>
-__device__ __forceinline__ void pi_at(bool general, bool pr, double2 dLx, double2 dLy, double2 dLz,
-                                      cplx<R>* P, R* lq_sqrt) {
-  const cplx<R> Lx = cvt<R>(dLx), Ly = cvt<R>(dLy), Lz = cvt<R>(dLz);
+__device__ __forceinline__ void pi_from(bool general, bool pr, cplx<R> Lx, cplx<R> Ly, cplx<R> Lz, cplx<R>* P) {
   const R Lq = cabs2(Lx) + cabs2(Ly) + cabs2(Lz);
   cplx<R> p1[3], p2[3];
   if (!general) {
@@ -81,7 +81,7 @@ __device__ __forceinline__ void pi_at(bool general, bool pr, double2 dLx, double
     const cplx<R> t2 = mk<R>(Lx.x - al * Lz.x, Lx.y - al * Lz.y);
     const cplx<R> t3 = mk<R>(al * Ly.x - be * Lx.x, al * Ly.y - be * Lx.y);
     const R n2 = cabs2(t1) + cabs2(t2) + cabs2(t3);
-    const R i1 = (R)1 / sqrt(n2 * Lq), i2 = (R)1 / sqrt(n2);
+    const R i2 = rsqrt(n2), i1 = i2 * rsqrt(Lq);
     // t x conj(Lambda)
     p1[0] = cscale(csub(cmul(t3, cconj(Ly)), cmul(t2, cconj(Lz))), i1);
     p1[1] = cscale(csub(cmul(t1, cconj(Lz)), cmul(t3, cconj(Lx))), i1);
@@ -94,8 +94,7 @@ __device__ __forceinline__ void pi_at(bool general, bool pr, double2 dLx, double
     // 3*Lq - |Ls|^2 (the reference's normaliser, …Lambdas.cu:450-451) written as
     // |Lx-Ly|^2 + |Ly-Lz|^2 + |Lz-Lx|^2: the same number without cancellation
     const R d2 = cabs2(csub(Lx, Ly)) + cabs2(csub(Ly, Lz)) + cabs2(csub(Lz, Lx));
-    const R d1 = Lq * d2;
-    const R i1 = (R)1 / sqrt(d1), i2 = (R)1 / sqrt(d2);
+    const R i2 = rsqrt(d2), i1 = i2 * rsqrt(Lq);
     const cplx<R> cs = cconj(Ls);
     p1[0] = cscale(csub(mk<R>(Lq, 0), cmul(Lx, cs)), i1);
     p1[1] = cscale(csub(mk<R>(Lq, 0), cmul(Ly, cs)), i1);
@@ -117,7 +116,6 @@ __device__ __forceinline__ void pi_at(bool general, bool pr, double2 dLx, double
       P[3 + c] = cconj(p1[c]);
     }
   }
-  if (lq_sqrt) *lq_sqrt = sqrt(Lq);
 }
 
 // sqrt(Lambda_q) at full frequency index fi, in FP64 (invAr scaling,

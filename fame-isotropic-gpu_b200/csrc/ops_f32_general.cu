@@ -1,0 +1,15 @@
+// Operator stage kernels, FP32, General lattices, radices 2, 3, 4, 5, 8.
+#include "op_kernels.cuh"
+
+namespace fame {
+template __global__ void k_plane_inv<float, true, IN_CG, false, false, DynGeom>(PlaneInArgs<float>);
+template __global__ void k_plane_inv<float, true, IN_VEC, false, false, DynGeom>(PlaneInArgs<float>);
+template __global__ void k_plane_inv<float, true, IN_VEC, true, false, DynGeom>(PlaneInArgs<float>);
+template __global__ void k_pencil<float, true, PEN_QBQ, false, DynGeom>(PencilArgs<float>);
+template __global__ void k_pencil<float, true, PEN_QR_OUT, false, DynGeom>(PencilArgs<float>);
+template __global__ void k_pencil<float, true, PEN_QRS_IN, false, DynGeom>(PencilArgs<float>);
+template __global__ void k_plane_fwd<float, true, EPI_CG, false, false, DynGeom>(PlaneOutArgs<float>);
+template __global__ void k_plane_fwd<float, true, EPI_OUT, false, false, DynGeom>(PlaneOutArgs<float>);
+template __global__ void k_plane_fwd<float, true, EPI_OUT, true, false, DynGeom>(PlaneOutArgs<float>);
+FAME_DEFINE_LAUNCH_GETTER(launches_ops_f32_general)
+}  // namespace fame

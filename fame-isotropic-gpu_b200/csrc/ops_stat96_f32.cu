@@ -1,0 +1,12 @@
+// Operator stage kernels with the compile-time 96 x 96 x 96 geometry (cubic Simple
+// lattice at Nx = 96), FP32: the CG and refinement hot path and the operator benchmark.
+#include "op_kernels.cuh"
+
+namespace fame {
+template __global__ void k_plane_inv<float, false, IN_CG, false, false, Stat96>(PlaneInArgs<float>);
+template __global__ void k_plane_inv<float, false, IN_VEC, false, false, Stat96>(PlaneInArgs<float>);
+template __global__ void k_pencil<float, false, PEN_QBQ, false, Stat96>(PencilArgs<float>);
+template __global__ void k_plane_fwd<float, false, EPI_CG, false, false, Stat96>(PlaneOutArgs<float>);
+template __global__ void k_plane_fwd<float, false, EPI_OUT, false, false, Stat96>(PlaneOutArgs<float>);
+FAME_DEFINE_LAUNCH_GETTER(launches_ops_stat96_f32)
+}  // namespace fame

@@ -15,7 +15,7 @@
 #include <tuple>
 #include <vector>
 
-#include "kernels.cuh"
+#include "state.cuh"
 
 namespace fame {
 

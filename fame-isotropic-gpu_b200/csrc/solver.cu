@@ -21,10 +21,23 @@
 #include <utility>
 
 #include "../../include/fame_b200.h"
+#include "op_kernels_decl.h"
 #include "program.h"
 #include "solver_kernels.cuh"
 
 namespace fame {
+
+unsigned long long launches_ops_f32_simple();
+unsigned long long launches_ops_f32_general();
+unsigned long long launches_ops_f64_simple();
+unsigned long long launches_ops_f64_general();
+unsigned long long launches_ops_f32_simple_rare();
+unsigned long long launches_ops_f32_general_rare();
+unsigned long long launches_ops_f64_simple_rare();
+unsigned long long launches_ops_f64_general_rare();
+unsigned long long launches_ops_stat96_f32();
+unsigned long long launches_ops_stat96_f64();
+FAME_DEFINE_LAUNCH_GETTER(launches_solver)
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -53,25 +66,6 @@ static bool factorize(int n, AxisPlan& p) {
     p.npass = 0;
   }
   return m == 1;
-}
-
-static void init_fft_constants() {
-  static bool done = false;
-  if (done) return;
-  auto fill = [](const void* sym_c, const void* sym_s, int r) {
-    std::vector<double> c(r), s(r);
-    for (int m = 0; m < r; m++) {
-      c[m] = cos(2.0 * M_PI * m / r);
-      s[m] = sin(2.0 * M_PI * m / r);
-    }
-    FAME_CK(cudaMemcpyToSymbol(sym_c, c.data(), r * sizeof(double)));
-    FAME_CK(cudaMemcpyToSymbol(sym_s, s.data(), r * sizeof(double)));
-  };
-  fill(c_cos5, c_sin5, 5);
-  fill(c_cos7, c_sin7, 7);
-  fill(c_cos11, c_sin11, 11);
-  fill(c_cos13, c_sin13, 13);
-  done = true;
 }
 
 // ------------------------------------------------------------------ device buffers
@@ -103,6 +97,8 @@ struct fame_ctx {
   Geom g;
   cudaStream_t stream = nullptr;
   int plane_threads = 512;
+  bool rare = false;    // some axis length has a factor outside {2, 3, 4, 5, 8}
+  bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   bool have_eps = false;
   // persistent data
   DBuf<double2> tw64;
@@ -135,10 +131,8 @@ static int vec_blocks(const fame_ctx* c, int nslots) {
   return (int)std::max<long>(1, std::min(b, cap));
 }
 
-template <typename R> static size_t plane_smem(const Geom& g) {
-  return sizeof(cplx<R>) * ((size_t)g.P + g.Lf + g.Lm);
-}
-template <typename R> static int pencil_tw() { return sizeof(R) == 8 ? 16 : 32; }
+template <typename R> static size_t plane_smem(const Geom& g) { return plane_smem_bytes<R>(g.Lf, g.Lm, g.S); }
+template <typename R> static int pencil_tw() { return PencilTW<R>::v; }
 template <typename R> static size_t pencil_smem(const Geom& g) {
   return sizeof(cplx<R>) * ((size_t)g.Ls * pencil_tw<R>() + g.Ls);
 }
@@ -195,11 +189,13 @@ struct Ops {
     const size_t sm = plane_smem<R>(g());
     dim3 grid(3 * g().Ls, nvec, nslots);
     if (g().general) {
-      auto k = k_plane_inv<R, true, IN, PR>;
+      auto k = c->rare ? k_plane_inv<R, true, IN, PR, true, DynGeom> : k_plane_inv<R, true, IN, PR, false, DynGeom>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     } else {
-      auto k = k_plane_inv<R, false, IN, PR>;
+      auto k = c->rare ? k_plane_inv<R, false, IN, PR, true, DynGeom> : k_plane_inv<R, false, IN, PR, false, DynGeom>;
+      if constexpr (kStatInv<R, IN, PR>)
+        if (c->stat96) k = k_plane_inv<R, false, IN, PR, false, Stat96>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     }
@@ -226,13 +222,15 @@ struct Ops {
     const int nft = (g().Lf + a.TW - 1) / a.TW;
     dim3 grid(g().Lm * nft, 3 * nvec, nslots);
     if (g().general) {
-      auto k = k_pencil<R, true, MODE>;
+      auto k = c->rare ? k_pencil<R, true, MODE, true, DynGeom> : k_pencil<R, true, MODE, false, DynGeom>;
       allow_smem(k, sm);
-      P.launch(k, grid, dim3(256), sm, a);
+      P.launch(k, grid, dim3(kPencilThreads), sm, a);
     } else {
-      auto k = k_pencil<R, false, MODE>;
+      auto k = c->rare ? k_pencil<R, false, MODE, true, DynGeom> : k_pencil<R, false, MODE, false, DynGeom>;
+      if constexpr (kStatPen<R, MODE>)
+        if (c->stat96) k = k_pencil<R, false, MODE, false, Stat96>;
       allow_smem(k, sm);
-      P.launch(k, grid, dim3(256), sm, a);
+      P.launch(k, grid, dim3(kPencilThreads), sm, a);
     }
   }
 
@@ -261,11 +259,13 @@ struct Ops {
     const size_t sm = plane_smem<R>(g());
     dim3 grid(3 * g().Ls, nvec, nslots);
     if (g().general) {
-      auto k = k_plane_fwd<R, true, EPI, PR>;
+      auto k = c->rare ? k_plane_fwd<R, true, EPI, PR, true, DynGeom> : k_plane_fwd<R, true, EPI, PR, false, DynGeom>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     } else {
-      auto k = k_plane_fwd<R, false, EPI, PR>;
+      auto k = c->rare ? k_plane_fwd<R, false, EPI, PR, true, DynGeom> : k_plane_fwd<R, false, EPI, PR, false, DynGeom>;
+      if constexpr (kStatFwd<R, EPI, PR>)
+        if (c->stat96) k = k_plane_fwd<R, false, EPI, PR, false, Stat96>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     }
@@ -306,12 +306,15 @@ static int setup_geom(fame_ctx* c) {
     g.Lf = g.Nz;
   }
   g.P = g.Lm * g.Lf;
+  g.S = g.Lf | 1;
   if (!factorize(g.Lf, g.pf) || !factorize(g.Lm, g.pm) || !factorize(g.Ls, g.ps)) {
     set_err("axis length needs more than 10 FFT passes");
     return FAME_ERR_UNSUPPORTED;
   }
+  c->rare = !(plan_is_common(g.pf) && plan_is_common(g.pm) && plan_is_common(g.ps));
   // the whole plane must fit one CTA's shared memory (FP64 copy)
   c->plane_threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
+  c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96 && c->plane_threads == kPlaneThreads;
   if (plane_smem<double>(g) > 227 * 1024) {
     set_err("plane " + std::to_string(g.Lm) + "x" + std::to_string(g.Lf) + " exceeds one CTA");
     return FAME_ERR_UNSUPPORTED;
@@ -706,7 +709,6 @@ int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out) {
     c->device = device;
     c->lat = *lat;
     FAME_CK(cudaSetDevice(device));
-    init_fft_constants();
     int rc = setup_geom(c);
     if (rc) {
       delete c;
@@ -1115,7 +1117,10 @@ int fame_launch_count(fame_ctx* c, unsigned long long* out) {
   try {
     FAME_CK(cudaSetDevice(c->device));
     FAME_CK(cudaStreamSynchronize(c->stream));
-    FAME_CK(cudaMemcpyFromSymbol(out, g_launches, sizeof(unsigned long long)));
+    *out = launches_solver() + launches_ops_f32_simple() + launches_ops_f32_general() + launches_ops_f64_simple() +
+           launches_ops_f64_general() + launches_ops_f32_simple_rare() + launches_ops_f32_general_rare() +
+           launches_ops_f64_simple_rare() + launches_ops_f64_general_rare() + launches_ops_stat96_f32() +
+           launches_ops_stat96_f64();
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;

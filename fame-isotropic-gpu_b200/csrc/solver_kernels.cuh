@@ -1,8 +1,61 @@
 // CG, invAr and FP64 Lanczos kernels.
 #pragma once
-#include "kernels.cuh"
+#include "state.cuh"
 
 namespace fame {
+
+// ------------------------------------------------------------------ tables
+// Per-k tables (FAME_Main/FAME_Matrix_Lambdas.cu:77-244 Simple, :288-489 General)
+// computed on the device: one thread per table entry, FP64 sincospi.
+__global__ void k_tables(Geom g, const Slot* slots, double2* tabs, double m1, double m2, double m3) {
+  FAME_COUNT_LAUNCH();
+  const int slot = blockIdx.y;
+  const Slot sl = slots[slot];
+  double2* t = tabs + (size_t)slot * g.tab_stride;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
+  if (!g.general) {
+    // Lambda_d[n] = (e^{i 2 pi (n + theta_d)/N_d} - 1)/h_d,  D_d[n] = e^{i 2 pi theta_d n / N_d}
+    if (i < Nx) {
+      double2 e = expipi(2.0 * (i + sl.th[0]) / Nx);
+      t[g.oLx + i] = make_double2((e.x - 1.0) / g.hx, e.y / g.hx);
+      t[g.oDx + i] = expipi(2.0 * sl.th[0] * i / Nx);
+    }
+    if (i < Ny) {
+      double2 e = expipi(2.0 * (i + sl.th[1]) / Ny);
+      t[g.oLy + i] = make_double2((e.x - 1.0) / g.hy, e.y / g.hy);
+      t[g.oDy + i] = expipi(2.0 * sl.th[1] * i / Ny);
+    }
+    if (i < Nz) {
+      double2 e = expipi(2.0 * (i + sl.th[2]) / Nz);
+      t[g.oLz + i] = make_double2((e.x - 1.0) / g.hz, e.y / g.hz);
+      t[g.oDz + i] = expipi(2.0 * sl.th[2] * i / Nz);
+    }
+  } else {
+    const double c1 = (m1 * m3) / ((double)Ny * Nx) - (m2 / Nx);
+    const double c2 = -(m3 / Ny);
+    if (i < Nx) {
+      double2 e = expipi(2.0 * (i + sl.th[0]) / Nx);
+      t[g.oLx + i] = make_double2((e.x - 1.0) / g.hx, e.y / g.hx);
+      t[g.oDkx + i] = expipi(2.0 * sl.th[0] * i / Nx);
+    }
+    if (i < Nx * Ny) {
+      const int x = i / Ny, y = i - x * Ny;
+      // mxy = -m1*x/Nx + y (…Lambdas.cu:333-335), Lambda_y over (x, y)
+      const double mxy = (-(m1 / Nx) * x) + y;
+      double2 e = expipi(2.0 * (mxy + sl.th[1]) / Ny);
+      t[g.oLy + i] = make_double2((e.x - 1.0) / g.hy, e.y / g.hy);
+      // D_ky[x, y] = e^{i 2 pi (theta_xy - m1 x / Nx) y / Ny} (…Lambdas.cu:382-388)
+      t[g.oDky + i] = expipi(2.0 * (sl.th[1] + x * (-m1 / Nx)) * y / Ny);
+      // phase base of Lambda_z and D_kz: phi = (theta_xyz + c1 x + c2 y)
+      const double ph = sl.th[2] + c1 * x + c2 * y;
+      t[g.oExy + i] = expipi(2.0 * ph / Nz);
+      t[g.oPhi + i] = make_double2(ph, 0.0);
+    }
+    if (i < Nz) t[g.oWz + i] = expipi(2.0 * i / Nz);
+  }
+}
+
 
 // Global index of reduced element i (0 <= i < 2*Nd) to its full frequency index.
 __device__ __forceinline__ int full_index(int i, int Nd, int off) { return (i < Nd ? i : i - Nd) + off; }

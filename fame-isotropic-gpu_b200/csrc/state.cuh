@@ -1,0 +1,162 @@
+// State, loop conditions and kernel argument structs shared by the operator
+// kernels (op_kernels.cuh) and the solver kernels (solver_kernels.cuh).
+#pragma once
+#include "operator.cuh"
+
+namespace fame {
+
+// complex elements a thread holds in registers during one FFT pass (per precision)
+template <typename R> struct Emax;
+template <> struct Emax<float> { static constexpr int v = 16; };
+template <> struct Emax<double> { static constexpr int v = 8; };
+// fast-axis positions per pencil CTA: 256-byte rows
+template <typename R> struct PencilTW { static constexpr int v = 256 / (int)sizeof(cplx<R>); };
+
+// ------------------------------------------------------------------ state
+struct CgState {
+  double r1, r0, beta;       // ||r||^2 now / before, r1/r0
+  double a_re, a_im;         // CG step a = r1 / <p, Ap>
+  double r1_0, tol2;         // initial ||r||^2, stop threshold on ||r||^2
+  int iter;                  // the reference's counter k (starts at 1, CG.cu:301)
+  int active;
+  int maxit;
+  int total;                 // CG products accumulated for the profile counter
+  // outer iterative refinement (mixed precision)
+  double rr, scale;          // ||b - A y||^2, 1/||b - A y|| used to scale the FP32 rhs
+  int outer, outer_active, outer_max, outer_total;
+};
+
+struct LzState {
+  int converged;
+  int restarts;
+  int nconv;
+  int pad;
+};
+
+// Condition of one CUDA-graph WHILE node (in host-driven mode only `flag` is used).
+// Every loop is fail-safe: the first kernel of the body clears the condition, the
+// deciding kernel sets it again only while work remains and the loop's trip count
+// (counted on the device) is below `cap`; hitting the cap records an overflow in
+// trips[1] and ends the loop, so no data-dependent loop can run unbounded.
+struct Cond {
+  cudaGraphConditionalHandle handle;
+  int* flag;
+  int* trips;  // [0] trips of the current loop, [1] overflow marker
+  int cap;
+};
+
+__device__ __forceinline__ void set_cond(const Cond& c, int v) {
+  if (!c.flag) return;
+  *c.flag = v;
+  if (c.handle) cudaGraphSetConditional(c.handle, (unsigned)v);
+}
+
+// decision at the end of a loop body
+__device__ __forceinline__ void decide_cond(const Cond& c, int any) {
+  if (c.trips) {
+    const int t = ++c.trips[0];
+    if (any && t >= c.cap) {
+      c.trips[1] = 1;
+      any = 0;
+    }
+  }
+  set_cond(c, any);
+}
+
+// before the loop: reset the trip counter and set the first decision
+__device__ __forceinline__ void start_cond(const Cond& c, int any) {
+  if (c.trips) c.trips[0] = 0;
+  set_cond(c, any);
+}
+
+// Ticket counter over the whole grid: true in exactly one CTA, the last one.
+__device__ __forceinline__ bool grid_last(unsigned* ctr, unsigned total) {
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ctr, 1u) == total - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    *ctr = 0u;
+  }
+  return last;
+}
+
+// D_kz(x, y, z) = e^{i 2 pi phi(x,y) z / Nz} (…Lambdas.cu:389-400)
+template <typename R>
+__device__ __forceinline__ cplx<R> dkz_at(const Geom& g, const double2* tab, int x, int y, int z) {
+  const double ph = tab[g.oPhi + x * g.Ny + y].x;
+  if constexpr (sizeof(R) == 8) {
+    // exact argument reduction of ph*z/Nz: the integer part of ph*z contributes 2*pi*n
+    return expipi(2.0 * ph * z / g.Nz);
+  } else {
+    return to_f(expipi(2.0 * ph * z / g.Nz));
+  }
+}
+
+// ------------------------------------------------------------------ plane stage
+enum InMode { IN_VEC = 0, IN_CG = 1, IN_REFINE = 2 };
+enum EpiMode { EPI_OUT = 0, EPI_CG = 1, EPI_RESID = 2 };
+enum PencilMode { PEN_QBQ = 0, PEN_QR_OUT = 1, PEN_QRS_IN = 2 };
+
+template <typename R>
+struct PlaneInArgs {
+  Geom g;
+  const Slot* slots;
+  const double2* tabs;
+  const cplx<R>* tw;      // forward twiddle tables, R precision
+  long vstride;           // per-slot stride of reduced vectors (elements)
+  long fstride;           // per-slot stride of 3N fields (elements)
+  int vec_per_slot;       // number of vectors per slot (batched Qr over bands)
+  const cplx<R>* in;      // IN_VEC: reduced input
+  cplx<R>* p;             // IN_CG: search direction (updated in place)
+  const cplx<R>* r;       // IN_CG: residual
+  CgState* cg;            // IN_CG / IN_REFINE
+  double2* y64;           // IN_REFINE: FP64 accumulated solution (updated)
+  const float2* x32;      // IN_REFINE: FP32 correction
+  int sigma;              // IN_VEC: multiply the input by sqrt(Lambda_q) first (Sigma, …_Isotropic.cu:109)
+  cplx<R>* T;             // output field (3 components)
+  Cond reset;             // loop condition cleared by this kernel when it starts a loop body
+};
+
+template <typename R>
+struct PencilArgs {
+  Geom g;
+  const Slot* slots;
+  const double2* tabs;
+  const cplx<R>* tw;
+  long fstride;
+  int vec_per_slot;
+  cplx<R>* T;              // field in frequency-plane layout (in/out)
+  const R* invB;           // PEN_QBQ: 1/eps per edge (3N, spatial layout); PEN_QR_OUT: optional
+  cplx<R>* out;            // PEN_QR_OUT: spatial field out (3N per vector)
+  const cplx<R>* in;       // PEN_QRS_IN: spatial field in
+  const CgState* cg;       // optional activity gate
+  int gate;                // 0 none, 1 CG active, 2 outer refinement active
+  int TW;                  // fast positions per CTA
+};
+
+template <typename R>
+struct PlaneOutArgs {
+  Geom g;
+  const Slot* slots;
+  const double2* tabs;
+  const cplx<R>* tw;
+  long vstride, fstride;
+  int vec_per_slot;
+  const cplx<R>* T;        // field after the slow-axis forward pass
+  cplx<R>* out;            // EPI_OUT: reduced output; EPI_CG: Ap; EPI_RESID: r (FP64)
+  const cplx<R>* p;        // EPI_CG: p for <p, Ap>
+  const cplx<R>* b;        // EPI_RESID: right-hand side
+  CgState* cg;
+  double* partials;        // [nslots][blocks per slot][NV]
+  unsigned* counters;      // [nslots] ticket counters, plus [nslots] = grid counter
+  Cond cond;               // EPI_RESID: outer WHILE condition
+  int nslots;
+  double tol2;             // EPI_RESID: absolute tolerance^2 on ||b - A y||
+};
+
+}  // namespace fame
