@@ -1,0 +1,336 @@
+// fame_qbq_static: Q_r^* B^{-1} Q_r in FP64 with no device allocation.
+//
+// Callers that cannot allocate device memory use this entry point: a host
+// framework that owns the whole device budget through its own pool (the
+// reference's FAME_Main_Code allocates its work arrays up front), and code that
+// runs where cudaMalloc is not allowed or must not block other streams (cudaMalloc
+// and cudaFree synchronise the device).  It needs no fame_ctx, whose creation
+// allocates the twiddle, table and workspace buffers of the solver.
+//
+// Scratch: one file-scope device array of kScratchBytes (4 MiB).  A call lays out
+// in it the k-point slot, the FFT twiddles, the Lambda/D_k tables and the
+// 3-component intermediate field T (3N complex doubles, 48 B per grid point), so
+// grids up to about 85,000 points fit; larger grids are rejected with
+// FAME_ERR_UNSUPPORTED and a message giving the bytes needed.
+//
+// Sharing: every call on every stream of a device uses the same array, and the
+// array keeps what the last call left in it.  Nothing in it has to start at zero:
+// each call writes the slot, twiddles, tables and T before any kernel reads them.
+// Two calls that may overlap in time (different streams, or different host threads
+// on one stream without ordering) race on the array; the caller serialises them.
+//
+// Set-up: the first call on a device, with that device current, looks up the
+// array's address with cudaGetSymbolAddress (once per device, checked; the address
+// is cached).  Make that first call before any stream capture.  Every call also
+// sets the dynamic shared-memory limit of the stage kernels it launches
+// (cudaFuncSetAttribute, which allocates nothing).
+//
+// Errors are reported by the return code and the text of fame_last_error().
+//
+// The computation is the one of fame_apply(FAME_OP_QBQ, FAME_FP64): the same
+// plane / pencil / plane kernels and the same table kernel, launched on the
+// caller's stream; only where their scratch lives differs.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+
+#include "../../include/fame_b200.h"
+#include "op_kernels_decl.h"
+
+namespace fame {
+
+// defined with the solver (solver_kernels.cuh, solver.cu)
+__global__ void k_tables(Geom g, const Slot* slots, double2* tabs, double m1, double m2, double m3);
+void set_last_error(const std::string& s);
+
+namespace {
+
+constexpr size_t kScratchBytes = FAME_QBQ_STATIC_SCRATCH_BYTES;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_qbq_scratch[kScratchBytes];
+
+// per-device set-up: address of the scratch array
+std::mutex g_setup_mu;
+void* g_scratch_ptr[kMaxDevices];
+
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// The slot and the forward twiddles e^{-2 pi i m / n} of the three axes.
+__global__ void k_static_prep(Slot sl, Geom g, Slot* slot, double2* tw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *slot = sl;
+  const int n[3] = {g.Lf, g.Lm, g.Ls};
+  const int o[3] = {g.twf, g.twm, g.tws};
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    if (i < n[a]) {
+      double s, c;
+      sincospi(2.0 * i / n[a], &s, &c);
+      tw[o[a] + i] = make_double2(c, -s);
+    }
+}
+
+bool factor_axis(int n, AxisPlan& p) {
+  // radix order of the solver's plans: 8, 4, 2, 5, 3, 7, 11, 13, then larger primes
+  p.n = n;
+  p.npass = 0;
+  int m = n;
+  const int order[] = {8, 4, 2, 5, 3, 7, 11, 13};
+  for (int r : order)
+    while (m % r == 0) {
+      if (p.npass >= kMaxPasses) return false;
+      p.radix[p.npass++] = r;
+      m /= r;
+    }
+  for (int q = 17; m > 1 && q <= m; q++)
+    while (m % q == 0) {
+      if (p.npass >= kMaxPasses) return false;
+      p.radix[p.npass++] = q;
+      m /= q;
+    }
+  return m == 1;
+}
+
+// Geometry of the lattice (the layout the solver's context sets up).
+int make_geom(const fame_lattice& L, Geom& g, bool& rare, int& threads) {
+  memset(&g, 0, sizeof(g));
+  g.Nx = L.grid[0];
+  g.Ny = L.grid[1];
+  g.Nz = L.grid[2];
+  if (g.Nx < 2 || g.Ny < 2 || g.Nz < 2) {
+    set_last_error("grid dimensions must be >= 2");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const long N = (long)g.Nx * g.Ny * g.Nz;
+  if (N > (1L << 24)) {
+    set_last_error("grid too large");
+    return FAME_ERR_UNSUPPORTED;
+  }
+  g.N = (int)N;
+  g.general = L.simple ? 0 : 1;
+  g.hx = L.mesh_len[0];
+  g.hy = L.mesh_len[1];
+  g.hz = L.mesh_len[2];
+  g.Ls = g.general ? g.Nx : g.Nz;
+  g.Lm = g.Ny;
+  g.Lf = g.general ? g.Nz : g.Nx;
+  g.P = g.Lm * g.Lf;
+  g.S = g.Lf | 1;
+  if (!factor_axis(g.Lf, g.pf) || !factor_axis(g.Lm, g.pm) || !factor_axis(g.Ls, g.ps)) {
+    set_last_error("axis length needs more than 10 FFT passes");
+    return FAME_ERR_UNSUPPORTED;
+  }
+  rare = !(plan_is_common(g.pf) && plan_is_common(g.pm) && plan_is_common(g.ps));
+  threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
+  if (plane_smem_bytes<double>(g.Lf, g.Lm, g.S) > 227 * 1024) {
+    set_last_error("plane exceeds one CTA");
+    return FAME_ERR_UNSUPPORTED;
+  }
+  int o = 0;
+  if (!g.general) {
+    g.oLx = o; o += g.Nx;
+    g.oLy = o; o += g.Ny;
+    g.oLz = o; o += g.Nz;
+    g.oDx = o; o += g.Nx;
+    g.oDy = o; o += g.Ny;
+    g.oDz = o; o += g.Nz;
+  } else {
+    g.oLx = o; o += g.Nx;
+    g.oLy = o; o += g.Nx * g.Ny;
+    g.oExy = o; o += g.Nx * g.Ny;
+    g.oWz = o; o += g.Nz;
+    g.oDky = o; o += g.Nx * g.Ny;
+    g.oPhi = o; o += g.Nx * g.Ny;
+    g.oDkx = o; o += g.Nx;
+  }
+  g.tab_stride = (o + 7) / 8 * 8;
+  g.twf = 0;
+  g.twm = g.Lf;
+  g.tws = g.Lf + g.Lm;
+  return FAME_OK;
+}
+
+// theta_x, theta_y(xy), theta_z(xyz) of a k-point (FAME_Main/FAME_Matrix_Lambdas.cu:43-70)
+void make_thetas(const fame_lattice& L, const double* k, double th[3]) {
+  const double* a = L.lattice_vec_a;
+  auto dot = [&](const double* v) { return k[0] * v[0] + k[1] * v[1] + k[2] * v[2]; };
+  th[0] = dot(a);
+  if (L.simple) {
+    th[1] = dot(a + 3);
+    th[2] = dot(a + 6);
+    return;
+  }
+  double c1 = 0.0;
+  if (a[3] > 0)
+    c1 = -(double)L.m[0] / (double)L.grid[0];
+  else if (a[3] < 0)
+    c1 = 1. - (double)L.m[0] / (double)L.grid[0];
+  const double c2 = (double)L.m[2] / (double)L.grid[1];
+  const double c3 = (double)L.m[1] / (double)L.grid[0];
+  double a2h[3], a3h[3];
+  for (int i = 0; i < 3; i++) a2h[i] = c1 * a[i] + a[3 + i];
+  for (int i = 0; i < 3; i++) a3h[i] = a[6 + i] - c2 * a2h[i] - c3 * a[i] + L.t1[i];
+  th[1] = dot(a2h);
+  th[2] = dot(a3h);
+}
+
+template <typename K> cudaError_t raise_smem(K* k, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <bool GEN, bool RARE>
+cudaError_t launch_qbq(const Geom& g, int threads, const Slot* slot, const double2* tabs, const double2* tw,
+                       const double2* x, const double* invB, double2* T, double2* y, cudaStream_t st) {
+  const long M = 2L * g.N, F = 3L * g.N;
+  auto kin = k_plane_inv<double, GEN, IN_VEC, false, RARE, DynGeom>;
+  auto kpen = k_pencil<double, GEN, PEN_QBQ, RARE, DynGeom>;
+  auto kout = k_plane_fwd<double, GEN, EPI_OUT, false, RARE, DynGeom>;
+  const size_t sm_plane = plane_smem_bytes<double>(g.Lf, g.Lm, g.S);
+  const int TW = PencilTW<double>::v;
+  const size_t sm_pen = sizeof(double2) * ((size_t)g.Ls * TW + g.Ls);
+  cudaError_t e;
+  if ((e = raise_smem(kin, sm_plane)) != cudaSuccess) return e;
+  if ((e = raise_smem(kpen, sm_pen)) != cudaSuccess) return e;
+  if ((e = raise_smem(kout, sm_plane)) != cudaSuccess) return e;
+
+  PlaneInArgs<double> ai;
+  memset(&ai, 0, sizeof(ai));
+  ai.g = g;
+  ai.slots = slot;
+  ai.tabs = tabs;
+  ai.tw = tw;
+  ai.vstride = M;
+  ai.fstride = F;
+  ai.vec_per_slot = 1;
+  ai.in = x;
+  ai.T = T;
+  kin<<<dim3(3 * g.Ls, 1, 1), dim3(threads), sm_plane, st>>>(ai);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+  PencilArgs<double> ap;
+  memset(&ap, 0, sizeof(ap));
+  ap.g = g;
+  ap.slots = slot;
+  ap.tabs = tabs;
+  ap.tw = tw;
+  ap.fstride = F;
+  ap.vec_per_slot = 1;
+  ap.T = T;
+  ap.invB = invB;
+  ap.TW = TW;
+  const int nft = (g.Lf + TW - 1) / TW;
+  kpen<<<dim3(g.Lm * nft, 3, 1), dim3(kPencilThreads), sm_pen, st>>>(ap);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+  PlaneOutArgs<double> ao;
+  memset(&ao, 0, sizeof(ao));
+  ao.g = g;
+  ao.slots = slot;
+  ao.tabs = tabs;
+  ao.tw = tw;
+  ao.vstride = M;
+  ao.fstride = F;
+  ao.vec_per_slot = 1;
+  ao.T = T;
+  ao.out = y;
+  ao.nslots = 1;
+  kout<<<dim3(3 * g.Ls, 1, 1), dim3(threads), sm_plane, st>>>(ao);
+  return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace fame
+
+using namespace fame;
+
+extern "C" {
+
+int fame_qbq_static(const fame_lattice* lat, const double* k, const double* inv_b, const void* x, void* y,
+                    void* stream) {
+  if (!lat || !k || !inv_b || !x || !y) {
+    set_last_error("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  Geom g;
+  bool rare = false;
+  int threads = 0;
+  int rc = make_geom(*lat, g, rare, threads);
+  if (rc != FAME_OK) return rc;
+  const size_t off_tw = align256(sizeof(Slot));
+  const size_t off_tab = off_tw + align256(sizeof(double2) * (size_t)(g.Lf + g.Lm + g.Ls));
+  const size_t off_T = off_tab + align256(sizeof(double2) * (size_t)g.tab_stride);
+  const size_t need = off_T + sizeof(double2) * 3 * (size_t)g.N;
+  if (need > kScratchBytes) {
+    set_last_error("grid of " + std::to_string(g.N) + " points needs " + std::to_string(need) +
+            " bytes of scratch; the static array holds " + std::to_string(kScratchBytes));
+    return FAME_ERR_UNSUPPORTED;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    set_last_error(std::string("cudaGetDevice: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "device index out of range"));
+    return FAME_ERR_CUDA;
+  }
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (!g_scratch_ptr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_qbq_scratch);
+      if (e != cudaSuccess) {
+        set_last_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        return FAME_ERR_CUDA;
+      }
+      g_scratch_ptr[dev] = p;
+    }
+    base = (unsigned char*)g_scratch_ptr[dev];
+  }
+  Slot sl;
+  memset(&sl, 0, sizeof(sl));
+  make_thetas(*lat, k, sl.th);
+  const double nrm = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+  // Gamma point: Nd = N - 1 (FAME_Main/FAME_Matrix_Lambdas.cu:157 Simple, :406 General)
+  sl.Nd = nrm < (lat->simple ? 1e-4 : 1e-3) ? g.N - 1 : g.N;
+  sl.off = g.N - sl.Nd;
+  sl.active = 1;
+  Slot* slot = (Slot*)base;
+  double2* tw = (double2*)(base + off_tw);
+  double2* tabs = (double2*)(base + off_tab);
+  double2* T = (double2*)(base + off_T);
+  cudaStream_t st = (cudaStream_t)stream;
+
+  const int nprep = std::max({g.Lf, g.Lm, g.Ls, 1});
+  k_static_prep<<<(nprep + 255) / 256, 256, 0, st>>>(sl, g, slot, tw);
+  if ((e = cudaGetLastError()) != cudaSuccess) {
+    set_last_error(std::string("prep launch: ") + cudaGetErrorString(e));
+    return FAME_ERR_CUDA;
+  }
+  const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
+  k_tables<<<dim3((tmax + 255) / 256, 1), dim3(256), 0, st>>>(g, slot, tabs, (double)lat->m[0], (double)lat->m[1],
+                                                              (double)lat->m[2]);
+  if ((e = cudaGetLastError()) != cudaSuccess) {
+    set_last_error(std::string("table launch: ") + cudaGetErrorString(e));
+    return FAME_ERR_CUDA;
+  }
+  const double2* xd = (const double2*)x;
+  double2* yd = (double2*)y;
+  if (g.general)
+    e = rare ? launch_qbq<true, true>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
+             : launch_qbq<true, false>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st);
+  else
+    e = rare ? launch_qbq<false, true>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
+             : launch_qbq<false, false>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st);
+  if (e != cudaSuccess) {
+    set_last_error(std::string("QBQ launch: ") + cudaGetErrorString(e));
+    return FAME_ERR_CUDA;
+  }
+  return FAME_OK;
+}
+
+}  // extern "C"

@@ -41,6 +41,8 @@ FAME_DEFINE_LAUNCH_GETTER(launches_solver)
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
+// error text of the entry points defined in other translation units
+void set_last_error(const std::string& s) { g_err = s; }
 
 // ------------------------------------------------------------------ FFT plans
 static bool factorize(int n, AxisPlan& p) {

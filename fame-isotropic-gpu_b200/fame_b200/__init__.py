@@ -29,7 +29,8 @@ OP_QR, OP_QRS, OP_QBQ, OP_PR, OP_PRS, OP_INVAR = range(6)
 # every symbol declared in include/fame_b200.h
 EXPORTS = ("fame_ctx_create", "fame_ctx_destroy", "fame_set_eps", "fame_set_material", "fame_solve_kpoints",
            "fame_apply", "fame_adjoint", "fame_ctx_sizes", "fame_last_error", "fame_version", "fame_ctx_stream",
-           "fame_launch_count", "fame_bench_qbq")
+           "fame_launch_count", "fame_bench_qbq", "fame_qbq_static")
+QBQ_STATIC_SCRATCH_BYTES = 4 << 20  # FAME_QBQ_STATIC_SCRATCH_BYTES
 
 
 class FameError(RuntimeError):
@@ -81,10 +82,11 @@ def load():
     lib.fame_ctx_stream.restype = C.c_void_p
     lib.fame_launch_count.argtypes = [P, C.POINTER(C.c_ulonglong)]
     lib.fame_bench_qbq.argtypes = [P, D, C.c_int, C.c_int, D, D]
+    lib.fame_qbq_static.argtypes = [C.POINTER(Lattice), D, P, P, P, P]
     lib.fame_last_error.restype = C.c_char_p
     lib.fame_version.restype = C.c_char_p
     for fn in ("fame_ctx_create", "fame_set_eps", "fame_set_material", "fame_solve_kpoints", "fame_apply",
-               "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq"):
+               "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq", "fame_qbq_static"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib
@@ -212,6 +214,16 @@ class Context:
         g = np.zeros((nw, self.N))
         _check(load().fame_adjoint(self._h, _dptr(f), e.ctypes.data_as(C.POINTER(C.c_double)), nw, 1, _dptr(g)))
         return g
+
+
+def qbq_static(lattice, k, inv_b, x, y, stream=0):
+    """Q_r^* B^-1 Q_r in FP64 through fame_qbq_static (no device allocation, no
+    context): lattice from make_lattice, inv_b (3N float64), x and y (2*Nd
+    complex128) torch CUDA tensors; enqueued on `stream` (a cudaStream_t as int,
+    0 = legacy default stream), not synchronised."""
+    kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+    _check(load().fame_qbq_static(C.byref(lattice), _dptr(kk), C.c_void_p(inv_b.data_ptr()),
+                                  C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(stream)))
 
 
 def version():

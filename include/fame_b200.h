@@ -150,6 +150,28 @@ int fame_bench_qbq(fame_ctx* ctx, const double* k, int precision, int reps, doub
 /* Grid size N and maximum reduced size 2N of the context, for buffer sizing. */
 int fame_ctx_sizes(const fame_ctx* ctx, long long* N_out);
 
+/* Bytes of the fixed device scratch array behind fame_qbq_static. */
+#define FAME_QBQ_STATIC_SCRATCH_BYTES (4u << 20)
+
+/* Q_r^* B^-1 Q_r in FP64 at one k-point with no device allocation and no context.
+ * No counterpart in the reference (it allocates its work arrays in FAME_Main_Code);
+ * this is for callers that own all device memory through their own pool or must
+ * not call cudaMalloc/cudaFree (which synchronise the device).
+ *   lat     host lattice description (same as fame_ctx_create)
+ *   k_xyz   host wave vector (3 doubles)
+ *   inv_b   device, 3N doubles: 1/eps per edge (x, y, z components, spatial layout)
+ *   x, y    device, 2*Nd complex128 each (Nd = N, or N-1 at the Gamma point)
+ *   stream  a cudaStream_t (NULL: the legacy default stream); the call only
+ *           enqueues work and returns without synchronising.
+ * Scratch is one static device array of FAME_QBQ_STATIC_SCRATCH_BYTES per device
+ * (48 bytes per grid point plus tables: grids up to about 85,000 points); larger
+ * grids return FAME_ERR_UNSUPPORTED.  Every call shares that array and leaves its
+ * contents behind (nothing in it has to start at zero); calls that can overlap in
+ * time race on it, so the caller serialises them.  The first call on a device
+ * looks up the array's address; make it before any stream capture. */
+int fame_qbq_static(const fame_lattice* lat, const double* k_xyz, const double* inv_b, const void* x, void* y,
+                    void* stream);
+
 const char* fame_last_error(void);
 const char* fame_version(void);
 
