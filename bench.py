@@ -3,7 +3,8 @@
 
 Workload: simple cubic lattice a=1, grid 96^3, one dielectric sphere (r=0.25a,
 eps=13) in eps=1, 10 bands, Lanczos restart dimension 40, Lanczos and CG
-tolerances 1e-10 (relative residual of every band checked <= 1e-6), the
+tolerances 1e-12 (the reference's defaults; relative residual of every band
+checked <= 1e-6), the
 reference's default band path GXMGRX|MR with part_num=4 (20 k-points).  The k
 path and the material map are the reference preprocessing outputs committed in
 tests/golden/sc96_pre.npz (synthetic crystal; no dataset involved).
@@ -40,7 +41,8 @@ sys.path.insert(0, os.path.join(ROOT, "fame-isotropic-gpu_b200"))
 METRIC = "k-points/s at 96^3, 10 bands, resid 1e-6: batched FP32 vs plain FP64, 1 B200"
 WORKLOAD = "sc96"
 NWANT, NSTEP = 10, 40
-TOLS = dict(es_tol=1e-10, ls_tol=1e-10, es_maxit=100, ls_maxit=1000)
+# the reference's default solver tolerances (its Popt.txt): Lanczos and CG 1e-12
+TOLS = dict(es_tol=1e-12, ls_tol=1e-12, es_maxit=100, ls_maxit=1000)
 
 
 def load_workload():
@@ -148,7 +150,7 @@ def rank_kpoints(W, rank):
 
 def cpu_baseline(W, es_mean, counters):
     """The oracle (numpy/scipy FP64 restatement of the reference method) timed on the
-    host cores: one A_r^-1 application (full CG to 1e-10) at a non-Gamma k of the
+    host cores: one A_r^-1 application (full CG to the bench tolerance) at a non-Gamma k of the
     path, scaled by the mean A_r^-1 count per k-point of this run."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import fame_oracle as fo
@@ -192,6 +194,8 @@ def run_ours(args):
     ctx.set_material(W["binout"], W["material_num"], W["eps_in"], W["eps_out"])
     N = int(np.prod(W["grid"]))
     kp = rank_kpoints(W, rank)
+    if args.nk:
+        kp = kp[: args.nk]
     nk = kp.shape[0]
     prec = fb.MIXED if args.precision == "mixed" else fb.FP64
     params = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=prec, batch=args.batch, **TOLS)
@@ -233,10 +237,12 @@ def run_ours(args):
     relres_max = float(np.max(out["relres"]))
     fr = out["freq"]
     ref_err = None
-    refp = os.path.join(ROOT, "tests", "golden", f"{WORKLOAD}_ref.json")
+    # reference frequencies at the same tolerance when a fixture exists for it
+    refp = os.path.join(ROOT, "tests", "golden", f"{WORKLOAD}_t12_ref.json" if TOLS["es_tol"] == 1e-12
+                        else f"{WORKLOAD}_ref.json")
     if rank == 0 and os.path.exists(refp):
         ref = json.load(open(refp))
-        rf = np.array([r["freq"] for r in ref["kpoints"]])
+        rf = np.array([r["freq"] for r in ref["kpoints"]])[: fr.shape[0]]
         nz = rf > 0
         ref_err = float(np.max(np.abs(fr[nz] - rf[nz]) / rf[nz]))
     counters = out["counters"]
@@ -275,9 +281,22 @@ def run_ours(args):
         ev1.synchronize()
         t64 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist)
         nz = o64["freq"] > 0
-        fp64 = {"value": nk * ws / t64, "unit": "k-points/s", "speedup_mixed_over_fp64": round(value / (nk * ws / t64), 3),
+        fp64 = {"value": nk * ws / t64, "unit": "k-points/s", "batch": args.batch or "auto", "graph": True,
+                "speedup_mixed_over_fp64": round(value / (nk * ws / t64), 3),
                 "max_rel_freq_diff_mixed_vs_fp64": float(np.max(np.abs(fr[nz] - o64["freq"][nz]) / o64["freq"][nz])),
                 "max_relres_fp64": float(np.max(o64["relres"]))}
+        # the plain form: FP64, one k-point at a time, loops driven by the host
+        # (the reference's structure), on the first args.plain_nk k-points
+        pp = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=fb.FP64, batch=1, use_graph=0, **TOLS)
+        kpp = kp[: max(1, args.plain_nk)]
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        ctx.solve(kpp, pp)
+        ev1.record(stream)
+        ev1.synchronize()
+        tpp = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist)
+        fp64["one_k_at_a_time_host_loops"] = {"value": kpp.shape[0] * ws / tpp, "kpoints": int(kpp.shape[0]),
+                                              "speedup_mixed_over_it": round(value / (kpp.shape[0] * ws / tpp), 3)}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(W, es_mean, counters)
@@ -288,7 +307,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 operator/CG + f64 refinement/Lanczos"
             if prec == fb.MIXED else "f64", "data": "synthetic (reference preprocessing of a synthetic SC crystal)",
             "config": {"workload": "SC a=1, 96^3, sphere r=0.25 eps=13 in eps=1, 10 bands, nstep 40, "
-                                   "tol 1e-10, path GXMGRX|MR part_num=4 (20 k-points per GPU)",
+                                   f"tol {TOLS['es_tol']:g}, path GXMGRX|MR part_num=4 ({nk} k-points per GPU)",
                        "grid": list(W["grid"]), "kpoints_per_gpu": nk, "precision": args.precision,
                        "batch": args.batch or "auto", "graph": True, "parallelism": f"k-sharding x{ws}",
                        "l2": "inputs exceed L2 per step (>1000 CG iterations per step)"},
@@ -305,6 +324,21 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_qbq(args):
+    """Q_r^* B^-1 Q_r applies alone at 96^3 (one k off Gamma), each preceded by a
+    256 MiB L2 flush: the small case the kernel profiles in profiles/ capture."""
+    import fame_b200 as fb
+    W = load_workload()
+    ctx = fb.Context(W["grid"], W["mesh_len"], W["lattice_vec_a"], W["simple"], W["m"], W["t1"])
+    ctx.set_material(W["binout"], W["material_num"], W["eps_in"], W["eps_out"])
+    prec = fb.MIXED if args.precision == "mixed" else fb.FP64
+    k = W["kpoints"][1]
+    ms, st = ctx.bench_qbq(k, prec, reps=max(1, args.steps))
+    print(json.dumps({"mode": "qbq", "precision": args.precision, "grid": list(W["grid"]), "reps": args.steps,
+                      "ms_per_apply": round(ms, 5), "stage_ms": [round(x, 5) for x in st]}), flush=True)
+    ctx.close()
+
+
 def edge_eps(W, N):
     """B (3N) from the material map with FAME_Matrix_B_Isotropic's last-wins rule."""
     B = np.full(3 * N, W["eps_out"])
@@ -318,7 +352,8 @@ def edge_eps(W, N):
 def run_reference(args):
     """The reference's own FP64 CUDA build (oracle/_ref/fame_ref_harness, compiled from
     the reference sources by oracle/build_ref.sh) through its own preprocessing and
-    FAME_Fast_Algorithms_Driver; each step = 4 k-points of the same 20-k path."""
+    FAME_Fast_Algorithms_Driver.  Each warm-up step is one k-point; each timed step
+    is the whole 20-k band path, one k at a time as the reference runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -328,11 +363,16 @@ def run_reference(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_inputs as ri
-    per_step = 4
-    n = (args.warmup + args.steps) * per_step
-    kidx = ",".join(str(i % 20) for i in range(n))
+    W = load_workload()
+    nkp = W["kpoints"].shape[0]
+    if args.nk:
+        nkp = min(nkp, args.nk)
+    per_step = nkp
+    order = [i % nkp for i in range(args.warmup)] + [i for _ in range(args.steps) for i in range(nkp)]
+    kidx = ",".join(str(i) for i in order)
     with tempfile.TemporaryDirectory() as d:
-        ri.make_workdir(WORKLOAD, d)
+        ri.make_workdir(WORKLOAD, d, es_tol=TOLS["es_tol"], es_maxit=TOLS["es_maxit"], ls_tol=TOLS["ls_tol"],
+                        ls_maxit=TOLS["ls_maxit"])
         out = os.path.join(d, "out.jsonl")
         with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
             rc = subprocess.run([harness, "solve", d, out, "--kidx", kidx], stdout=subprocess.DEVNULL,
@@ -341,7 +381,7 @@ def run_reference(args):
             print(json.dumps({"impl": "reference", "unavailable": f"reference build failed rc={rc.returncode}: {rc.stderr[-200:]}"}))
             return
         recs = [json.loads(l) for l in open(out)]
-    timed = recs[args.warmup * per_step:]
+    timed = recs[args.warmup:]
     t = sum(r["wall_s"] for r in timed)
     value = len(timed) / t
     line = {
@@ -349,8 +389,8 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": "SC a=1, 96^3, sphere r=0.25 eps=13 in eps=1, 10 bands, nstep 40, tol 1e-10, "
-                               "path GXMGRX|MR part_num=4", "grid": [96, 96, 96], "kpoints_per_step": per_step,
+        "config": {"workload": "SC a=1, 96^3, sphere r=0.25 eps=13 in eps=1, 10 bands, nstep 40, "
+                               f"tol {TOLS['es_tol']:g}, path GXMGRX|MR part_num=4", "grid": [96, 96, 96], "kpoints_per_step": per_step,
                    "parallelism": "none (the reference runs one GPU, one k at a time)"},
         "cpu_baseline": {"value": round(value, 4), "unit": "k-points/s", "cores": 1, "kind": "reference",
                          "sample": f"{len(timed)} k-points of the 96^3 path through the reference's own FP64 "
@@ -373,9 +413,17 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="solve", choices=["solve", "qbq"],
+                    help="qbq: only time Q_r^* B^-1 Q_r applies at 96^3 (--steps applies; for kernel profiles)")
+    ap.add_argument("--plain-nk", type=int, default=4, help="k-points of the one-at-a-time FP64 measurement")
+    ap.add_argument("--nk", type=int, default=0, help="solve only the first NK k-points (launch-list samples)")
+    ap.add_argument("--tol", type=float, default=TOLS["es_tol"], help="Lanczos and CG tolerance")
     args = ap.parse_args()
+    TOLS["es_tol"] = TOLS["ls_tol"] = args.tol
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "qbq":
+        return run_qbq(args)
     return run_ours(args)
 
 

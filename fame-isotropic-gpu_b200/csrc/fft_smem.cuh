@@ -141,6 +141,28 @@ template <typename R> struct Dft<R, 8> {
   }
 };
 
+// Radix 12 as a prime-factor (Good-Thomas) DFT 3 x 4, no internal twiddles:
+// input n = (4 n1 + 3 n2) mod 12, output k = (4 k1 + 9 k2) mod 12 with
+// k1 = k mod 3, k2 = k mod 4 (Chinese remainder map).
+template <typename R> struct Dft<R, 12> {
+  __device__ __forceinline__ static void run(cplx<R>* a, bool inv) {
+    cplx<R> y[4][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+#pragma unroll
+      for (int n1 = 0; n1 < 3; n1++) y[n2][n1] = a[(4 * n1 + 3 * n2) % 12];
+      Dft<R, 3>::run(y[n2], inv);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+      cplx<R> z[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      Dft<R, 4>::run(z, inv);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; k2++) a[(4 * k1 + 9 * k2) % 12] = z[k2];
+    }
+  }
+};
+
 // Odd radix via symmetric pairs: X_t = a0 + sum_s c(ts) (a_s + a_{R-s})
 //                                       -/+ i sum_s s(ts) (a_s - a_{R-s}).
 template <typename R, int RAD> struct DftOdd {
@@ -343,9 +365,17 @@ __device__ __forceinline__ void fft_lines(cplx<R>* buf, const AxisPlan P, LineSe
 
 
 // ---------------------------------------------------------------- compile-time plans
-// Static factorisation of a line length into the inlined radices 8, 4, 2, 5, 3
-// (same order as the host's runtime plans).
+// Static plans: a two-pass split n = r0 * r1 with both radices in {4, 8, 12}
+// when one exists (fewest passes, each a single register-staged round), else the
+// greedy factorisation into 8, 4, 2, 5, 3 of the runtime plans.
+constexpr int kSplit[][2] = {{8, 12}, {12, 8}, {8, 8}, {4, 12}, {12, 12}, {4, 8}, {8, 4}, {4, 4}};
+constexpr int splan_split(int n) {
+  for (int i = 0; i < (int)(sizeof(kSplit) / sizeof(kSplit[0])); i++)
+    if (kSplit[i][0] * kSplit[i][1] == n) return i;
+  return -1;
+}
 constexpr int splan_count(int n) {
+  if (splan_split(n) >= 0) return 2;
   int c = 0;
   const int rs[5] = {8, 4, 2, 5, 3};
   for (int i = 0; i < 5; i++)
@@ -356,6 +386,7 @@ constexpr int splan_count(int n) {
   return n == 1 ? c : -1;
 }
 constexpr int splan_radix(int n, int p) {
+  if (splan_split(n) >= 0) return kSplit[splan_split(n)][p];
   const int rs[5] = {8, 4, 2, 5, 3};
   int c = 0;
   for (int i = 0; i < 5; i++)
@@ -423,12 +454,22 @@ __device__ __forceinline__ void spass(cplx<R>* buf, int ls, int es, const cplx<R
   }
 }
 
+// Butterflies a thread stages per round: enough that all NL lines fit one round
+// when T >= NL (T / NL threads per line), capped by EMAX elements in registers.
+constexpr int smaxb(int N, int NL, int T, int EMAX, int RAD) {
+  const int nb = N / RAD;
+  const int tpl = T / NL > 0 ? T / NL : 1;
+  const int want = (nb + tpl - 1) / tpl;
+  const int cap = EMAX / RAD > 0 ? EMAX / RAD : 1;
+  return want < cap ? want : cap;
+}
+
 template <typename R, int N, int NL, int T, int EMAX, int P = 0, int NS = 1>
 __device__ __forceinline__ void sfft(cplx<R>* buf, int ls, int es, const cplx<R>* tw, bool inv) {
-  static_assert(splan_count(N) > 0, "line length must factor into 2, 3, 4, 5, 8");
+  static_assert(splan_count(N) > 0, "line length must factor into 2, 3, 4, 5, 8, 12");
   if constexpr (P < splan_count(N)) {
     constexpr int RAD = splan_radix(N, P);
-    constexpr int MB = RAD == 5 ? (EMAX / 5 > 2 ? 2 : (EMAX / 5 > 0 ? EMAX / 5 : 1)) : (EMAX / RAD > 0 ? EMAX / RAD : 1);
+    constexpr int MB = smaxb(N, NL, T, EMAX, RAD);
     spass<R, N, NL, T, NS, RAD, MB>(buf, ls, es, tw, inv);
     sfft<R, N, NL, T, EMAX, P + 1, NS * RAD>(buf, ls, es, tw, inv);
   }

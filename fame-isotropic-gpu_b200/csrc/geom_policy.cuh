@@ -10,11 +10,14 @@
 
 namespace fame {
 
-constexpr int kPlaneThreads = 512;   // threads of a plane CTA with a static geometry
-constexpr int kPencilThreads = 256;  // threads of a pencil CTA
+constexpr int kPlaneThreads = 512;      // most threads of a plane CTA (runtime geometry)
+constexpr int kStatPlaneThreads = 384;  // threads of a plane CTA with a static geometry
+constexpr int kPencilThreads = 256;     // threads of a pencil CTA
 
 struct DynGeom {
   static constexpr bool kStatic = false;
+  static constexpr int kMaxPlaneThreads = kPlaneThreads;
+  __device__ __forceinline__ static int plane_threads() { return blockDim.x; }
   __device__ __forceinline__ static int Lf(const Geom& g) { return g.Lf; }
   __device__ __forceinline__ static int Lm(const Geom& g) { return g.Lm; }
   __device__ __forceinline__ static int Ls(const Geom& g) { return g.Ls; }
@@ -36,10 +39,19 @@ struct DynGeom {
   }
 };
 
+// elements a thread stages per round in the static passes
+template <typename R> struct SEmax;
+template <> struct SEmax<float> { static constexpr int v = 24; };
+template <> struct SEmax<double> { static constexpr int v = 12; };
+
 template <int LF, int LM, int LSL>
 struct StatGeom {
   static constexpr bool kStatic = true;
   static constexpr int kS = LF | 1;
+  // 384 = 4 threads per line of a 96 x 96 plane: every pass of the 8 x 12 plan
+  // is one round with all threads busy
+  static constexpr int kMaxPlaneThreads = kStatPlaneThreads;
+  __device__ __forceinline__ static constexpr int plane_threads() { return kStatPlaneThreads; }
   __device__ __forceinline__ static constexpr int Lf(const Geom&) { return LF; }
   __device__ __forceinline__ static constexpr int Lm(const Geom&) { return LM; }
   __device__ __forceinline__ static constexpr int Ls(const Geom&) { return LSL; }
@@ -49,12 +61,12 @@ struct StatGeom {
   template <typename R, bool RARE>
   __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom&, bool fast, const cplx<R>* tw,
                                                    bool inv) {
-    sfft<R, LF, LM, kPlaneThreads, Emax<R>::v>(b, fast ? kS : 1, fast ? 1 : kS, tw, inv);
+    sfft<R, LF, LM, kStatPlaneThreads, SEmax<R>::v>(b, fast ? kS : 1, fast ? 1 : kS, tw, inv);
   }
   template <typename R, bool RARE>
   __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom&, const cplx<R>* tw, bool inv) {
     constexpr int TW = PencilTW<R>::v;
-    sfft<R, LSL, TW, kPencilThreads, Emax<R>::v>(b, 1, TW, tw, inv);
+    sfft<R, LSL, TW, kPencilThreads, SEmax<R>::v>(b, 1, TW, tw, inv);
   }
 };
 

@@ -29,7 +29,7 @@ __device__ __forceinline__ void lam_elem(const Geom& g, const double2* tab, cons
 
 // One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
 template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, 1)
     k_plane_inv(PlaneInArgs<R> a) {
   FAME_COUNT_LAUNCH();
   if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(a.reset, 0);
@@ -58,11 +58,11 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
     }
   }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
-  for (int i = threadIdx.x; i < Lf; i += blockDim.x) {
+  for (int i = threadIdx.x; i < Lf; i += GP::plane_threads()) {
     twf[i] = a.tw[g.twf + i];
     if constexpr (!GEN) lx[i] = cvt<R>(tab[g.oLx + i]);
   }
-  for (int i = threadIdx.x; i < Lm; i += blockDim.x) {
+  for (int i = threadIdx.x; i < Lm; i += GP::plane_threads()) {
     twm[i] = a.tw[g.twm + i];
     if constexpr (!GEN) ly[i] = cvt<R>(tab[g.oLy + i]);
   }
@@ -83,7 +83,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
     beta = (R)st->beta;
   }
   if constexpr (IN == IN_REFINE) rscale = (R)(1.0 / st->scale);
-  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+  for (int e = e0 + threadIdx.x; e < e1; e += GP::plane_threads()) {
     const int fi = s * P + e;
     const int m = e / Lf, f = e - m * Lf;
     cplx<R> v[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
@@ -142,7 +142,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
     if constexpr (GEN) {
       // x D_kz(x,y,z) after the z (fast) pass (FAME_FFT_CUDA.cu:278, kernel :452-487),
       // x D_ky(x,y) after the y (mid) pass (FAME_FFT_CUDA.cu:284, kernel :367-404)
-      for (int e = threadIdx.x; e < P; e += blockDim.x) {
+      for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
         const int m = e / Lf, f = e - m * Lf;
         const int q = m * S + f;
         plane[q] = cmul(plane[q], ax == 0 ? dkz_at<R>(g, tab, s, m, f) : cvt<R>(tab[g.oDky + s * g.Ny + m]));
@@ -151,7 +151,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
     }
   }
   cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
-  for (int e = threadIdx.x; e < P; e += blockDim.x) {
+  for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
     const int m = e / Lf;
     T[e] = plane[e + m * (S - Lf)];
   }
@@ -180,10 +180,10 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
   const int f0 = (blockIdx.x - m * nft) * TW;
   const int tw_n = min(TW, Lf - f0);
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
-  for (int i = threadIdx.x; i < Ls; i += blockDim.x) tws[i] = a.tw[g.tws + i];
+  for (int i = threadIdx.x; i < Ls; i += kPencilThreads) tws[i] = a.tw[g.tws + i];
   const long fb = (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N;
   // ---- load
-  for (int q = threadIdx.x; q < Ls * TW; q += blockDim.x) {
+  for (int q = threadIdx.x; q < Ls * TW; q += kPencilThreads) {
     const int s = q / TW, f = q - s * TW;
     cplx<R> v = mk<R>(0, 0);
     if (f < tw_n) {
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
     GP::template fft_slow<R, RARE>(tile, g, tws, inv);
     if (MODE != PEN_QRS_IN && dir == 0) {
       const R invN = (R)(1.0 / g.N);
-      for (int q = threadIdx.x; q < Ls * TW; q += blockDim.x) {
+      for (int q = threadIdx.x; q < Ls * TW; q += kPencilThreads) {
         const int s = q / TW, f = q - s * TW;
         if (f < tw_n) {
           long sp;
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
     }
   }
   if constexpr (MODE == PEN_QBQ || MODE == PEN_QRS_IN) {
-    for (int q = threadIdx.x; q < Ls * TW; q += blockDim.x) {
+    for (int q = threadIdx.x; q < Ls * TW; q += kPencilThreads) {
       const int s = q / TW, f = q - s * TW;
       if (f < tw_n) a.T[fb + (long)s * P + m * Lf + f0 + f] = tile[q];
     }
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
 // ------------------------------------------------------------------ plane stage (forward)
 
 template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, 1)
     k_plane_fwd(PlaneOutArgs<R> a) {
   FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -284,17 +284,17 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
     return;
   }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
-  for (int i = threadIdx.x; i < Lf; i += blockDim.x) {
+  for (int i = threadIdx.x; i < Lf; i += GP::plane_threads()) {
     twf[i] = a.tw[g.twf + i];
     if constexpr (!GEN) lx[i] = cvt<R>(tab[g.oLx + i]);
   }
-  for (int i = threadIdx.x; i < Lm; i += blockDim.x) {
+  for (int i = threadIdx.x; i < Lm; i += GP::plane_threads()) {
     twm[i] = a.tw[g.twm + i];
     if constexpr (!GEN) ly[i] = cvt<R>(tab[g.oLy + i]);
   }
   const cplx<R> lz = GEN ? mk<R>(0, 0) : cvt<R>(tab[g.oLz + s]);
   const cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
-  for (int e = threadIdx.x; e < P; e += blockDim.x) {
+  for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
     const int m = e / Lf;
     plane[e + m * (S - Lf)] = T[e];
   }
@@ -305,7 +305,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
   for (int ax = 0; ax < 2; ax++) {
     const bool fast = GEN ? ax == 1 : ax == 0;
     if constexpr (GEN) {
-      for (int e = threadIdx.x; e < P; e += blockDim.x) {
+      for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
         const int m = e / Lf, f = e - m * Lf;
         const int q = m * S + f;
         plane[q] = cmul(plane[q], ax == 0 ? cvt<R>(cconj(tab[g.oDky + s * g.Ny + m]))
@@ -324,7 +324,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(512, 1)
   const int Nd = sl.Nd, off = sl.off;
   const long vb = (long)(slot * a.vec_per_slot + vec) * a.vstride;
   double acc[2] = {0.0, 0.0};
-  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+  for (int e = e0 + threadIdx.x; e < e1; e += GP::plane_threads()) {
     const int fi = s * P + e;
     if (fi < off) continue;
     const long i = fi - off;

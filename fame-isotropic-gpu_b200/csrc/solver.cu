@@ -196,10 +196,14 @@ struct Ops {
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     } else {
       auto k = c->rare ? k_plane_inv<R, false, IN, PR, true, DynGeom> : k_plane_inv<R, false, IN, PR, false, DynGeom>;
+      int nt = c->plane_threads;
       if constexpr (kStatInv<R, IN, PR>)
-        if (c->stat96) k = k_plane_inv<R, false, IN, PR, false, Stat96>;
+        if (c->stat96) {
+          k = k_plane_inv<R, false, IN, PR, false, Stat96>;
+          nt = kStatPlaneThreads;
+        }
       allow_smem(k, sm);
-      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+      P.launch(k, grid, dim3(nt), sm, a);
     }
   }
 
@@ -266,10 +270,14 @@ struct Ops {
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     } else {
       auto k = c->rare ? k_plane_fwd<R, false, EPI, PR, true, DynGeom> : k_plane_fwd<R, false, EPI, PR, false, DynGeom>;
+      int nt = c->plane_threads;
       if constexpr (kStatFwd<R, EPI, PR>)
-        if (c->stat96) k = k_plane_fwd<R, false, EPI, PR, false, Stat96>;
+        if (c->stat96) {
+          k = k_plane_fwd<R, false, EPI, PR, false, Stat96>;
+          nt = kStatPlaneThreads;
+        }
       allow_smem(k, sm);
-      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+      P.launch(k, grid, dim3(nt), sm, a);
     }
   }
 };
@@ -316,7 +324,7 @@ static int setup_geom(fame_ctx* c) {
   c->rare = !(plan_is_common(g.pf) && plan_is_common(g.pm) && plan_is_common(g.ps));
   // the whole plane must fit one CTA's shared memory (FP64 copy)
   c->plane_threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
-  c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96 && c->plane_threads == kPlaneThreads;
+  c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96;
   if (plane_smem<double>(g) > 227 * 1024) {
     set_err("plane " + std::to_string(g.Lm) + "x" + std::to_string(g.Lf) + " exceeds one CTA");
     return FAME_ERR_UNSUPPORTED;
@@ -581,7 +589,7 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
              c->b64.p, tol2, s.ls_maxit);
     P.while_loop(outer, [&] {
       P.launch(k_cg32_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), (const double2*)c->r64.p,
-               c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit, outer);
+               c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit, tol2, outer);
       P.while_loop(inner, [&] {
         o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr,
                                          inner);

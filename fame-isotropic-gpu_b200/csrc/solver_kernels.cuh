@@ -211,9 +211,12 @@ __global__ void __launch_bounds__(256) k_invar_pro(VecArgs va, LzArgs L, int j, 
 }
 
 // Start of one FP32 inner solve: r32 = (float)(r64 * scale), x32 = 0; stop when
-// ||r32||^2 <= tau^2 ||r32_0||^2 or after `maxit` products.
+// ||r32|| <= tau' ||r32_0|| or after `maxit` products, where tau' = max(tau,
+// ls_tol / (2 ||r64||)): a refinement step never reduces the residual further than
+// the outer tolerance needs (outer_tol2 = ls_tol^2).
 __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r64, float2* r32,
-                                                   float2* x32, double tau2, int maxit, Cond outer_reset) {
+                                                   float2* x32, double tau2, int maxit, double outer_tol2,
+                                                   Cond outer_reset) {
   FAME_COUNT_LAUNCH();
   if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(outer_reset, 0);
   const int slot = blockIdx.z;
@@ -237,10 +240,11 @@ __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r6
     if (slot_reduce<1>(acc, va.partials + (size_t)slot * gridDim.x, va.counters + slot, blockIdx.x,
                        gridDim.x, tot)) {
       if (threadIdx.x == 0) {
+        const double need = st->rr > 0 ? 0.25 * outer_tol2 / st->rr : 0.0;
         st->r1 = tot[0];
         st->r0 = tot[0];
         st->r1_0 = tot[0];
-        st->tol2 = tau2 * tot[0];
+        st->tol2 = (need > tau2 ? need : tau2) * tot[0];
         st->iter = 1;
         st->maxit = maxit;
         st->active = (tot[0] > st->tol2) && (1 <= maxit);

@@ -4,6 +4,8 @@
     python tests/golden/make_golden.py ref OUTDIR     # on a B200, runs the reference's
                                                       # FP64 CUDA solver (oracle/_ref)
     python tests/golden/make_golden.py condense OUTDIR
+    python tests/golden/make_golden.py ref-big OUTDIR       # on a B200: full-size runs
+    python tests/golden/make_golden.py condense-big OUTDIR
 
 `pre` runs the reference's preprocessing (FAME_Preprocessing) through
 oracle/_ref/fame_ref_harness for every named workload and stores its integer and
@@ -13,6 +15,9 @@ geometric outputs (grid, m1-m4, Omega, k path, Binout, ...) as <name>_pre.npz.
 metric band path, writing <name>_ref.jsonl (frequencies, counters, wall time per k)
 and <name>_apply.npz (reference Qr/Qrs/QBQ/invAr applied to seeded vectors) into
 OUTDIR; `condense OUTDIR` then writes the committed subset into tests/golden/.
+`ref-big` runs the full-size configurations (BIG_RUNS): the 96^3 band path at the
+reference's default tolerance 1e-12 and a few k-points of FCC 64, BCC 48 and hex
+128; `condense-big` writes their frequency and counter fixtures.
 """
 from __future__ import annotations
 
@@ -112,6 +117,46 @@ def do_ref(outdir):
 
 
 
+# Full-size runs: the 96^3 band path at the reference's default tolerances
+# (1e-12, its Popt.txt) and a few k-points of the FCC 64, BCC 48 and hex 128
+# configurations at 1e-10.  (name, fixture name, k indices, tolerance)
+BIG_RUNS = [
+    ("sc96", "sc96_t12", None, 1e-12),
+    ("fcc64", "fcc64", "0,1,2", 1e-10),
+    ("bcc48", "bcc48", "0,1,2", 1e-10),
+    ("hex128", "hex128", "1,2", 1e-10),
+]
+
+
+def do_ref_big(outdir):
+    os.makedirs(outdir, exist_ok=True)
+    for name, fix, kidx, tol in BIG_RUNS:
+        with tempfile.TemporaryDirectory() as d:
+            ri.make_workdir(name, d, es_tol=tol, ls_tol=tol)
+            out = os.path.join(outdir, f"{fix}_ref.jsonl")
+            cmd = [ri.REF_HARNESS, "solve", d, out]
+            if kidx:
+                cmd += ["--kidx", kidx]
+            with open(os.path.join(outdir, f"{fix}_ref.log"), "w") as log:
+                subprocess.run(cmd, check=True, stdout=log, stderr=subprocess.STDOUT)
+        print("done", fix, flush=True)
+
+
+def condense_big(src, dst=GOLDEN):
+    meta = open(os.path.join(src, "gpu.txt")).read().strip().splitlines()
+    for name, fix, kidx, tol in BIG_RUNS:
+        recs = [json.loads(l) for l in open(os.path.join(src, f"{fix}_ref.jsonl"))]
+        out = dict(workload=name, device=meta[1].split(",")[0], host_cores=int(meta[2]),
+                   note=f"reference FP64 CUDA build (oracle/_ref/fame_ref_harness solve), "
+                        f"es_tol=ls_tol={tol:g}, es_maxit=100, ls_maxit=1000",
+                   kidx=[int(v) for v in kidx.split(",")] if kidx else None, tol=tol,
+                   kpoints=[dict(k=r["k"], wave_vec=r["wave_vec"], Nd=r["Nd"], freq=r["freq"],
+                                 ls_iter=r["ls_iter"], es_iter=r["es_iter"], wall_s=r["wall_s"])
+                            for r in recs])
+        with open(os.path.join(dst, f"{fix}_ref.json"), "w") as f:
+            json.dump(out, f, indent=1)
+
+
 def condense(src, dst=GOLDEN):
     """Keeps the committed part of a `ref` run: all frequencies and counters, and
     the operator applications at k-points 0 (Gamma) and 1 only."""
@@ -143,5 +188,9 @@ if __name__ == "__main__":
         do_ref(sys.argv[2])
     elif sys.argv[1] == "condense":
         condense(sys.argv[2])
+    elif sys.argv[1] == "ref-big":
+        do_ref_big(sys.argv[2])
+    elif sys.argv[1] == "condense-big":
+        condense_big(sys.argv[2])
     else:
         raise SystemExit(__doc__)
