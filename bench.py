@@ -198,7 +198,8 @@ def run_ours(args):
         kp = kp[: args.nk]
     nk = kp.shape[0]
     prec = fb.MIXED if args.precision == "mixed" else fb.FP64
-    params = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=prec, batch=args.batch, **TOLS)
+    params = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=prec, batch=args.batch,
+                              use_graph=0 if args.no_graph else 1, **TOLS)
     stream = torch.cuda.ExternalStream(ctx.stream())
     out = None
     for _ in range(args.warmup):
@@ -250,7 +251,7 @@ def run_ours(args):
     ls_sum = int(sum(c["ls_iter"] for c in counters))
     # ---- roofline of the dominant kernel: one Q_r^* B^-1 Q_r apply (3 fused stages)
     hbm, src = peaks()
-    kq = kp[1]
+    kq = W["kpoints"][1]
     ms, stages = ctx.bench_qbq(kq, prec, reps=20)
     s = 8 if prec == fb.MIXED else 16
     r = 4 if prec == fb.MIXED else 8
@@ -309,7 +310,7 @@ def run_ours(args):
             "config": {"workload": "SC a=1, 96^3, sphere r=0.25 eps=13 in eps=1, 10 bands, nstep 40, "
                                    f"tol {TOLS['es_tol']:g}, path GXMGRX|MR part_num=4 ({nk} k-points per GPU)",
                        "grid": list(W["grid"]), "kpoints_per_gpu": nk, "precision": args.precision,
-                       "batch": args.batch or "auto", "graph": True, "parallelism": f"k-sharding x{ws}",
+                       "batch": args.batch or "auto", "graph": not args.no_graph, "parallelism": f"k-sharding x{ws}",
                        "l2": "inputs exceed L2 per step (>1000 CG iterations per step)"},
             "accuracy": {"max_relres": relres_max, "max_rel_err_vs_reference_fp64": ref_err,
                          "max_relerr_vs_fp64_rayleigh": float(np.max(out["relerr"]))},
@@ -415,6 +416,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="solve", choices=["solve", "qbq"],
                     help="qbq: only time Q_r^* B^-1 Q_r applies at 96^3 (--steps applies; for kernel profiles)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="host-driven loops instead of the CUDA graph (launch lists under ncu)")
     ap.add_argument("--plain-nk", type=int, default=4, help="k-points of the one-at-a-time FP64 measurement")
     ap.add_argument("--nk", type=int, default=0, help="solve only the first NK k-points (launch-list samples)")
     ap.add_argument("--tol", type=float, default=TOLS["es_tol"], help="Lanczos and CG tolerance")

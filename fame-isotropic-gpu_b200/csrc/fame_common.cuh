@@ -83,6 +83,30 @@ __device__ __forceinline__ float2 expipi(float x) {
   return make_float2(c, s);
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80+): the data never passes
+// through registers, so a thread keeps all its copies in flight at once.
+// cp_async_wait_all waits for this thread's copies; a __syncthreads() after it
+// publishes them to the CTA.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+// one element of 8 or 16 bytes
+template <typename T> __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  static_assert(sizeof(T) == 8 || sizeof(T) == 16, "8- or 16-byte elements");
+  if constexpr (sizeof(T) == 16)
+    cp_async16(smem, gmem);
+  else
+    cp_async8(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Kernels launched on the device, counted by each kernel's first thread.  Every
 // translation unit has its own counter; FAME_DEFINE_LAUNCH_GETTER exposes it.
 static __device__ unsigned long long g_launches;

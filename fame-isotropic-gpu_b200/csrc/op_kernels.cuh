@@ -167,8 +167,10 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
   const Geom& g = a.g;
   constexpr int TW = PencilTW<R>::v;
   const int Lf = GP::Lf(g), Ls = GP::Ls(g), P = GP::P(g);
-  cplx<R>* tile = reinterpret_cast<cplx<R>*>(smem_raw);  // [Ls][TW]
-  cplx<R>* tws = tile + Ls * TW;
+  // shared memory: tile [Ls][TW] | 1/eps tile [Ls][TW] (PEN_QBQ) | slow-axis twiddles [Ls]
+  cplx<R>* tile = reinterpret_cast<cplx<R>*>(smem_raw);
+  R* ibt = reinterpret_cast<R*>(tile + Ls * TW);
+  cplx<R>* tws = reinterpret_cast<cplx<R>*>(ibt + Ls * TW);
   const int slot = blockIdx.z;
   const Slot sl = a.slots[slot];
   if (!sl.active) return;
@@ -182,7 +184,22 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
   for (int i = threadIdx.x; i < Ls; i += kPencilThreads) tws[i] = a.tw[g.tws + i];
   const long fb = (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N;
-  // ---- load
+  // ---- load.  Full tiles of the Simple-lattice QBQ stream the field rows (TW
+  // contiguous elements at stride P) and the 1/eps rows straight into shared
+  // memory with 16-byte cp.async copies.
+  constexpr int CH = 16 / sizeof(cplx<R>);    // elements per 16-byte copy
+  constexpr int CHB = 16 / sizeof(R);         // 1/eps values per 16-byte copy
+  const bool async_tile = MODE == PEN_QBQ && !GEN && tw_n == TW && Lf % CHB == 0;
+  if (async_tile) {
+    for (int q = threadIdx.x; q < Ls * (TW / CH); q += kPencilThreads) {
+      const int s = q / (TW / CH), c = q - s * (TW / CH);
+      cp_async16(tile + s * TW + c * CH, a.T + fb + (long)s * P + m * Lf + f0 + c * CH);
+    }
+    for (int q = threadIdx.x; q < Ls * (TW / CHB); q += kPencilThreads) {
+      const int s = q / (TW / CHB), c = q - s * (TW / CHB);
+      cp_async16(ibt + s * TW + c * CHB, a.invB + (long)comp * g.N + (long)s * P + m * Lf + f0 + c * CHB);
+    }
+  } else {
   for (int q = threadIdx.x; q < Ls * TW; q += kPencilThreads) {
     const int s = q / TW, f = q - s * TW;
     cplx<R> v = mk<R>(0, 0);
@@ -206,6 +223,8 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
     }
     tile[q] = v;
   }
+  }
+  if (async_tile) cp_async_wait_all();
   __syncthreads();
   // QBQ: inverse, x B^{-1}/N, forward.  QR_OUT: inverse, x D/N (and B^{-1}), store.
   // QRS_IN: forward only.  One FFT call site (dir loop) for the register budget.
@@ -224,7 +243,8 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
           else
             sp = ((long)(f0 + f) * g.Ny + m) * g.Nx + s;
           if constexpr (MODE == PEN_QBQ) {
-            tile[q] = cscale(tile[q], a.invB[(long)comp * g.N + sp] * invN);
+            const R ib = async_tile ? ibt[q] : a.invB[(long)comp * g.N + sp];
+            tile[q] = cscale(tile[q], ib * invN);
           } else {
             cplx<R> d;
             if (!GEN)
@@ -296,8 +316,9 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   const cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
   for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
     const int m = e / Lf;
-    plane[e + m * (S - Lf)] = T[e];
+    cp_async_elem(plane + e + m * (S - Lf), T + e);
   }
+  cp_async_wait_all();
   __syncthreads();
   // forward 2-D transform.  General lattices (T*, FAME_FFT_CUDA.cu:297-319):
   // x conj(D_ky), y (mid) pass, x conj(D_kz), z (fast) pass.  Simple lattices:

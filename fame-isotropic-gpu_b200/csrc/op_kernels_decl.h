@@ -10,6 +10,12 @@ __host__ __device__ inline size_t plane_smem_bytes(int Lf, int Lm, int S) {
   return sizeof(cplx<R>) * ((size_t)Lm * S + 2 * (size_t)Lf + 2 * (size_t)Lm);
 }
 
+// shared memory of a pencil CTA: tile [Ls x TW] | 1/eps tile [Ls x TW] | twiddles [Ls]
+template <typename R>
+__host__ __device__ inline size_t pencil_smem_bytes(int Ls) {
+  return (sizeof(cplx<R>) + sizeof(R)) * (size_t)Ls * PencilTW<R>::v + sizeof(cplx<R>) * (size_t)Ls;
+}
+
 template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP> __global__ void k_plane_inv(PlaneInArgs<R> a);
 template <typename R, bool GEN, int MODE, bool RARE, class GP> __global__ void k_pencil(PencilArgs<R> a);
 template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP> __global__ void k_plane_fwd(PlaneOutArgs<R> a);

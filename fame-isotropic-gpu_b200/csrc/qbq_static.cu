@@ -193,7 +193,7 @@ cudaError_t launch_qbq(const Geom& g, int threads, const Slot* slot, const doubl
   auto kout = k_plane_fwd<double, GEN, EPI_OUT, false, RARE, DynGeom>;
   const size_t sm_plane = plane_smem_bytes<double>(g.Lf, g.Lm, g.S);
   const int TW = PencilTW<double>::v;
-  const size_t sm_pen = sizeof(double2) * ((size_t)g.Ls * TW + g.Ls);
+  const size_t sm_pen = pencil_smem_bytes<double>(g.Ls);
   cudaError_t e;
   if ((e = raise_smem(kin, sm_plane)) != cudaSuccess) return e;
   if ((e = raise_smem(kpen, sm_pen)) != cudaSuccess) return e;

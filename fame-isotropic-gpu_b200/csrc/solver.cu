@@ -135,9 +135,7 @@ static int vec_blocks(const fame_ctx* c, int nslots) {
 
 template <typename R> static size_t plane_smem(const Geom& g) { return plane_smem_bytes<R>(g.Lf, g.Lm, g.S); }
 template <typename R> static int pencil_tw() { return PencilTW<R>::v; }
-template <typename R> static size_t pencil_smem(const Geom& g) {
-  return sizeof(cplx<R>) * ((size_t)g.Ls * pencil_tw<R>() + g.Ls);
-}
+template <typename R> static size_t pencil_smem(const Geom& g) { return pencil_smem_bytes<R>(g.Ls); }
 
 template <typename K> static void allow_smem(K* k, size_t bytes) {
   if (bytes > 48 * 1024) FAME_CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
