@@ -17,6 +17,7 @@ constexpr int kPencilThreads = 256;     // threads of a pencil CTA
 struct DynGeom {
   static constexpr bool kStatic = false;
   static constexpr int kMaxPlaneThreads = kPlaneThreads;
+  static constexpr int kMinPlaneBlocks = 1;
   __device__ __forceinline__ static int plane_threads() { return blockDim.x; }
   __device__ __forceinline__ static int Lf(const Geom& g) { return g.Lf; }
   __device__ __forceinline__ static int Lm(const Geom& g) { return g.Lm; }
@@ -39,10 +40,14 @@ struct DynGeom {
   }
 };
 
-// elements a thread stages per round in the static passes
+// elements a thread stages per round in the static passes: plane passes (FP32 at
+// most 80 registers, two CTAs per SM) and pencil passes
 template <typename R> struct SEmax;
-template <> struct SEmax<float> { static constexpr int v = 24; };
+template <> struct SEmax<float> { static constexpr int v = 12; };
 template <> struct SEmax<double> { static constexpr int v = 12; };
+template <typename R> struct SPenEmax;
+template <> struct SPenEmax<float> { static constexpr int v = 24; };
+template <> struct SPenEmax<double> { static constexpr int v = 12; };
 
 template <int LF, int LM, int LSL>
 struct StatGeom {
@@ -51,6 +56,7 @@ struct StatGeom {
   // 384 = 4 threads per line of a 96 x 96 plane: every pass of the 8 x 12 plan
   // is one round with all threads busy
   static constexpr int kMaxPlaneThreads = kStatPlaneThreads;
+  static constexpr int kMinPlaneBlocks = 2;  // two FP32 plane CTAs per SM
   __device__ __forceinline__ static constexpr int plane_threads() { return kStatPlaneThreads; }
   __device__ __forceinline__ static constexpr int Lf(const Geom&) { return LF; }
   __device__ __forceinline__ static constexpr int Lm(const Geom&) { return LM; }
@@ -66,7 +72,7 @@ struct StatGeom {
   template <typename R, bool RARE>
   __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom&, const cplx<R>* tw, bool inv) {
     constexpr int TW = PencilTW<R>::v;
-    sfft<R, LSL, TW, kPencilThreads, SEmax<R>::v>(b, 1, TW, tw, inv);
+    sfft<R, LSL, TW, kPencilThreads, SPenEmax<R>::v>(b, 1, TW, tw, inv);
   }
 };
 

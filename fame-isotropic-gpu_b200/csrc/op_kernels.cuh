@@ -29,7 +29,7 @@ __device__ __forceinline__ void lam_elem(const Geom& g, const double2* tab, cons
 
 // One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
 template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, 1)
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, sizeof(R) == 4 ? GP::kMinPlaneBlocks : 1)
     k_plane_inv(PlaneInArgs<R> a) {
   FAME_COUNT_LAUNCH();
   if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(a.reset, 0);
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
 // ------------------------------------------------------------------ plane stage (forward)
 
 template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, 1)
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, sizeof(R) == 4 ? GP::kMinPlaneBlocks : 1)
     k_plane_fwd(PlaneOutArgs<R> a) {
   FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];
