@@ -315,7 +315,8 @@ def run_ours(args):
             "accuracy": {"max_relres": relres_max, "max_rel_err_vs_reference_fp64": ref_err,
                          "max_relerr_vs_fp64_rayleigh": float(np.max(out["relerr"]))},
             "counters": {"es_iter_mean": es_mean, "ls_iter_total": ls_sum,
-                         "restarts_total": int(sum(c["restarts"] for c in counters))},
+                         "restarts_total": int(sum(c["restarts"] for c in counters)),
+                         "fp64_refinements_total": int(sum(c["refine"] for c in counters))},
             "roofline": roof, "plain_fp64": fp64, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(),
         }

@@ -427,7 +427,7 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
   c->G.ensure((size_t)nslots * (nstep + 1) * (nwant + 1));
   c->stats.ensure((size_t)nslots * nwant * 8);
   c->map.ensure((size_t)nslots * (nstep + 1) + (size_t)nslots * (nwant + 1));
-  c->prof.ensure((size_t)nslots * 2);
+  c->prof.ensure((size_t)nslots * 3);
   c->status.ensure(nslots);
   c->flags.ensure(64);
   const int nphys = nstep + 1 + nwant + 1;
@@ -846,7 +846,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     s.vec = p.want_vectors ? 1 : 0;
     s.es_tol = p.es_tol;
     s.ls_tol = p.ls_tol;
-    s.inner_tol = p.inner_tol > 0 ? p.inner_tol : 1e-5;
+    s.inner_tol = p.inner_tol > 0 ? p.inner_tol : 2e-6;  // two FP64 refinement steps reach 1e-12
     s.inner_maxit = p.inner_maxit > 0 ? p.inner_maxit : 200;
     const bool graph = p.use_graph != 0;
     ensure_workspace(c, s.nslots, s.nstep, s.nwant, s.mixed, s.vec);
@@ -868,7 +868,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     std::vector<Slot> hs(s.nslots);
     std::vector<double> theta((size_t)s.nslots * s.nstep), stats((size_t)s.nslots * s.nwant * 4);
     std::vector<LzState> lz(s.nslots);
-    std::vector<int> prof(2 * s.nslots), status(s.nslots);
+    std::vector<int> prof(3 * s.nslots), status(s.nslots);
     for (int b0 = 0; b0 < nk; b0 += s.nslots) {
       const int nb = std::min(s.nslots, nk - b0);
       for (int q = 0; q < s.nslots; q++) {
@@ -942,12 +942,12 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
         }
         if (counters) {
           fame_kcounters& kc = counters[kk];
-          kc.ls_iter = prof[2 * q];
-          kc.es_iter = prof[2 * q + 1];
+          kc.ls_iter = prof[3 * q];
+          kc.es_iter = prof[3 * q + 1];
           kc.restarts = lz[q].restarts;
           kc.status = status[q] == 0 ? FAME_OK : FAME_ERR_NO_CONVERGENCE;
           kc.Nd = hs[q].Nd;
-          kc.pad = 0;
+          kc.refine = prof[3 * q + 2];
         }
         if (status[q] != 0) rc_all = FAME_ERR_NO_CONVERGENCE;
         if (s.vec) {

@@ -138,7 +138,7 @@ struct LzArgs {
   double* T1;              // [nslots][nstep]
   double* h;               // [nslots][nstep+2] reorthogonalisation coefficients
   LzState* lz;
-  int* prof;               // [nslots][2]: ls_iter, es_iter (reference Profile counters)
+  int* prof;               // [nslots][3]: ls_iter, es_iter (reference Profile counters), FP64 refinements
 };
 
 __device__ __forceinline__ double2* ucol(const LzArgs& L, int slot, int logical) {
@@ -292,8 +292,9 @@ __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, 
     if (threadIdx.x == 0) {
       L.T0[slot * L.nstep + j] = tot[0];
       const CgState* st = va.cg + slot;
-      L.prof[slot * 2 + 0] += MIXED ? st->total : st->iter;
-      L.prof[slot * 2 + 1] += 1;
+      L.prof[slot * 3 + 0] += MIXED ? st->total : st->iter;
+      L.prof[slot * 3 + 1] += 1;
+      if (MIXED) L.prof[slot * 3 + 2] += st->outer_total;
     }
   }
 }
@@ -447,8 +448,9 @@ __global__ void k_lz_init(VecArgs va, LzArgs L) {
     L.lz[slot].converged = 0;
     L.lz[slot].restarts = 0;
     L.lz[slot].nconv = 0;
-    L.prof[slot * 2] = 0;
-    L.prof[slot * 2 + 1] = 0;
+    L.prof[slot * 3] = 0;
+    L.prof[slot * 3 + 1] = 0;
+    L.prof[slot * 3 + 2] = 0;
   }
   if (!sl.active) return;
   double2* u = L.U + (size_t)slot * L.nphys * L.ustride;  // physical column 0 == logical 0

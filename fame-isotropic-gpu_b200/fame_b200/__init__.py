@@ -53,7 +53,7 @@ class SolverParams(C.Structure):
 
 class KCounters(C.Structure):
     _fields_ = [("ls_iter", C.c_int), ("es_iter", C.c_int), ("restarts", C.c_int), ("status", C.c_int),
-                ("Nd", C.c_int), ("pad", C.c_int)]
+                ("Nd", C.c_int), ("refine", C.c_int)]
 
 
 _lib = None
@@ -172,7 +172,7 @@ class Context:
                                        ev.ctypes.data_as(C.POINTER(C.c_double)) if ev is not None else None, cnt)
         out = dict(freq=freq, relres=rr, relerr=re, rc=rc,
                    counters=[dict(ls_iter=c.ls_iter, es_iter=c.es_iter, restarts=c.restarts, status=c.status,
-                                  Nd=c.Nd) for c in cnt])
+                                  Nd=c.Nd, refine=c.refine) for c in cnt])
         if ev is not None:
             out["evec"] = ev
         if rc not in (OK, ERR_NO_CONVERGENCE):

@@ -71,7 +71,7 @@ typedef struct {
   int precision;    /* FAME_FP64 or FAME_MIXED */
   int batch;        /* k-points in flight per launch (0 = automatic) */
   int use_graph;    /* 1 = run each batch as one CUDA graph (default), 0 = host-driven loop */
-  double inner_tol; /* FAME_MIXED: relative tolerance of each FP32 inner solve (0 = 1e-5) */
+  double inner_tol; /* FAME_MIXED: relative tolerance of each FP32 inner solve (0 = 2e-6) */
   int inner_maxit;  /* FAME_MIXED: products per FP32 inner solve (0 = 200) */
   int want_vectors; /* 1 = compute and return the eigenvectors E */
 } fame_solver_params;
@@ -84,7 +84,7 @@ typedef struct {
   int restarts;     /* Lanczos restarts */
   int status;       /* FAME_OK / FAME_ERR_NO_CONVERGENCE for this k */
   int Nd;           /* N or N-1 (Gamma point) */
-  int pad;
+  int refine;       /* FAME_MIXED: FP64 refinement steps (each one FP64 Q_r^* B^-1 Q_r); else 0 */
 } fame_kcounters;
 
 /* Create a context on `device` for one lattice/grid.  Allocates nothing per k yet. */
