@@ -259,7 +259,7 @@ def run_ours(args):
     achieved = alg / (ms * 1e-3) / 1e9
     stage_bytes = [(2 * N + 3 * N) * s, 6 * N * s + 3 * N * r, (3 * N + 2 * N) * s]
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "qbq_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "qbq_96cubed_traffic.json")
     if os.path.exists(tp):
         tj = json.load(open(tp)).get("fp32" if prec == fb.MIXED else "fp64")
         if tj and tj.get("grid") == list(W["grid"]):
