@@ -512,6 +512,22 @@ def solve_k(wave_vec, par, B, es, ls):
 
 
 # ------------------------------------------------------------------ material / B
+def hellmann_feynman_voxel_gradient(E, freq, B, N):
+    """d w_i / d eps_v for C^H C E = w^2 B E with one permittivity per voxel on its
+    three edges: -(w_i / 2) sum_c |E_i,c,v|^2 / (E_i^H B E_i).  E: (nwant, 3N),
+    freq: (nwant,), B: (3N,).  The reference has no adjoint; this is the textbook
+    first-order perturbation of a generalized Hermitian eigenvalue, used to check
+    the adjoint kernel against the reference's own eigenvectors."""
+    E = np.asarray(E).reshape(len(freq), 3 * N)
+    a2 = np.abs(E) ** 2
+    den = a2 @ B
+    g = a2[:, :N] + a2[:, N:2 * N] + a2[:, 2 * N:]
+    w = np.asarray(freq, dtype=float)
+    out = -(w / 2.0)[:, None] * g / den[:, None]
+    out[w <= 0] = 0.0
+    return out
+
+
 def matrix_B(binout, material_num, eps_in, eps_out, N):
     """FAME_Matrix_B_Isotropic (FAME_Main/FAME_Matrix_B_Isotropic.cu:4-74): the last
     matching material wins."""

@@ -6,6 +6,8 @@
     python tests/golden/make_golden.py condense OUTDIR
     python tests/golden/make_golden.py ref-big OUTDIR       # on a B200: full-size runs
     python tests/golden/make_golden.py condense-big OUTDIR
+    python tests/golden/make_golden.py ref-adjoint OUTDIR   # on a B200: adjoint config
+    python tests/golden/make_golden.py condense-adjoint OUTDIR
 
 `pre` runs the reference's preprocessing (FAME_Preprocessing) through
 oracle/_ref/fame_ref_harness for every named workload and stores its integer and
@@ -157,6 +159,55 @@ def condense_big(src, dst=GOLDEN):
             json.dump(out, f, indent=1)
 
 
+# Adjoint check configuration: simple cubic 32^3, one permittivity per voxel drawn
+# uniform in [1, 13] from numpy.random.default_rng(0), 8 bands at k = (0.25, 0, 0)
+# (Cartesian, without 2*pi), tolerances 1e-12.
+ADJ_SEED, ADJ_K, ADJ_NWANT, ADJ_TOL, ADJ_SAMPLES = 0, (0.25, 0.0, 0.0), 8, 1e-12, 1024
+
+
+def adjoint_eps(N):
+    return np.random.default_rng(ADJ_SEED).uniform(1.0, 13.0, N)
+
+
+def do_ref_adjoint(outdir):
+    """The reference's FP64 solve with the per-voxel permittivity written straight
+    into its B (fame_ref_harness --eps) and its eigenvectors saved (--evec)."""
+    os.makedirs(outdir, exist_ok=True)
+    g = np.load(os.path.join(GOLDEN, "sc32_pre.npz"))
+    N = int(np.prod(g["grid_nums"]))
+    e = adjoint_eps(N)
+    with tempfile.TemporaryDirectory() as d:
+        ri.make_workdir("sc32", d, es_tol=ADJ_TOL, ls_tol=ADJ_TOL, nwant=ADJ_NWANT)
+        np.concatenate([e, e, e]).astype("<f8").tofile(os.path.join(d, "eps.bin"))
+        with open(os.path.join(d, "k.txt"), "w") as f:
+            f.write("1\n%.17g %.17g %.17g\n" % ADJ_K)
+        with open(os.path.join(outdir, "sc32_adjoint_ref.log"), "w") as log:
+            subprocess.run([ri.REF_HARNESS, "solve", d, os.path.join(outdir, "sc32_adjoint_ref.jsonl"),
+                            "--k", os.path.join(d, "k.txt"), "--eps", os.path.join(d, "eps.bin"),
+                            "--evec", os.path.join(outdir, "sc32_adjoint_evec")],
+                           check=True, stdout=log, stderr=subprocess.STDOUT)
+    print("done sc32_adjoint", flush=True)
+
+
+def condense_adjoint(src, dst=GOLDEN):
+    """Frequencies and the Hellmann-Feynman gradient from the reference's eigenvectors:
+    full per-band sums and norms, and the values at ADJ_SAMPLES seeded voxels."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fame_oracle as fo
+    g = np.load(os.path.join(GOLDEN, "sc32_pre.npz"))
+    N = int(np.prod(g["grid_nums"]))
+    e = adjoint_eps(N)
+    B = np.concatenate([e, e, e])
+    rec = json.loads(open(os.path.join(src, "sc32_adjoint_ref.jsonl")).readline())
+    freq = np.array(rec["freq"])
+    E = np.fromfile(os.path.join(src, "sc32_adjoint_evec_k000.bin"), "<c16").reshape(ADJ_NWANT, 3 * N)
+    G = fo.hellmann_feynman_voxel_gradient(E, freq, B, N)
+    idx = np.sort(np.random.default_rng(ADJ_SEED + 1).choice(N, ADJ_SAMPLES, replace=False))
+    np.savez_compressed(os.path.join(dst, "sc32_adjoint_ref.npz"), freq=freq, idx=idx, grad=G[:, idx],
+                        grad_sum=G.sum(axis=1), grad_norm=np.linalg.norm(G, axis=1),
+                        es_iter=rec["es_iter"], ls_iter=rec["ls_iter"])
+
+
 def condense(src, dst=GOLDEN):
     """Keeps the committed part of a `ref` run: all frequencies and counters, and
     the operator applications at k-points 0 (Gamma) and 1 only."""
@@ -192,5 +243,9 @@ if __name__ == "__main__":
         do_ref_big(sys.argv[2])
     elif sys.argv[1] == "condense-big":
         condense_big(sys.argv[2])
+    elif sys.argv[1] == "ref-adjoint":
+        do_ref_adjoint(sys.argv[2])
+    elif sys.argv[1] == "condense-adjoint":
+        condense_adjoint(sys.argv[2])
     else:
         raise SystemExit(__doc__)
