@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* E
 // ||E||^2 per (slot, band) and the reference's scaling E *= ||E||
 // (FAME_Fast_Algorithms_Isotropic.cu:119-121).
 __global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, double2* E, long fstride,
-                                                          int nwant, long n3) {
+                                                          int nwant, long n3, double* norms) {
   FAME_COUNT_LAUNCH();
   const int band = blockIdx.x, slot = blockIdx.y;
   if (!slots[slot].active) return;
@@ -504,7 +504,10 @@ __global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, dou
   __shared__ double sred[32];
   block_reduce<1>(acc, sred);
   __shared__ double nrm;
-  if (threadIdx.x == 0) nrm = sqrt(acc[0]);
+  if (threadIdx.x == 0) {
+    nrm = sqrt(acc[0]);
+    norms[slot * nwant + band] = nrm;
+  }
   __syncthreads();
   const double s = nrm;
   for (long i = threadIdx.x; i < n3; i += blockDim.x) e[i] = cscale(e[i], s);
@@ -540,13 +543,15 @@ __global__ void __launch_bounds__(256) k_adj_grad(const double2* E, const double
 // ------------------------------------------------------------------ recording
 struct SolveCfg {
   int nslots, nstep, nwant, es_maxit, ls_maxit, mixed, vec, inner_maxit;
+  int enorm;  // restore E (norms only) for the reference-scaled residual
   double es_tol, ls_tol, inner_tol;
 };
 
 static std::string cfg_key(const SolveCfg& s, bool graph) {
   char b[256];
-  snprintf(b, sizeof b, "%d/%d/%d/%d/%d/%d/%d/%d/%.17g/%.17g/%.17g/%d", s.nslots, s.nstep, s.nwant, s.es_maxit,
-           s.ls_maxit, s.mixed, s.vec, s.inner_maxit, s.es_tol, s.ls_tol, s.inner_tol, (int)graph);
+  snprintf(b, sizeof b, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%.17g/%.17g/%.17g/%d", s.nslots, s.nstep, s.nwant,
+           s.es_maxit, s.ls_maxit, s.mixed, s.vec, s.enorm, s.inner_maxit, s.es_tol, s.ls_tol, s.inner_tol,
+           (int)graph);
   return b;
 }
 
@@ -671,12 +676,13 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
   P.launch(k_band_stats, dim3(1, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{}),
            (const double2*)c->EV.p, (const double2*)c->AV.p, M, s.nwant, (const double*)c->theta.p, s.nstep,
            c->stats.p);
-  if (s.vec) {
-    // E = B^{-1} Q_r (Sigma ev), scaled by its norm (FAME_Fast_Algorithms_Isotropic.cu:107-122)
+  if (s.vec || s.enorm) {
+    // E = B^{-1} Q_r (Sigma ev), scaled by its norm (FAME_Fast_Algorithms_Isotropic.cu:107-122);
+    // the norms go after the band statistics
     o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
     o.pencil<double, PEN_QR_OUT>(c->Tb.p, s.nwant, F, c->invB64.p, 0, c->E.p);
     P.launch(k_band_norm_scale, dim3(s.nwant, s.nslots), dim3(1024), 0, (const Slot*)c->slots.p, c->E.p, F,
-             s.nwant, F);
+             s.nwant, F, c->stats.p + (size_t)s.nslots * s.nwant * 4);
   }
 }
 
@@ -813,8 +819,8 @@ int fame_set_material(fame_ctx* c, const int* binout, int material_num, const do
 }
 
 int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solver_params* prm,
-                       double* freq_out, double* relres_out, double* relerr_out, double* evec_out,
-                       fame_kcounters* counters) {
+                       double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
+                       double* evec_out, fame_kcounters* counters) {
   if (!c || !k_xyz || !prm || !freq_out || nk <= 0) {
     set_err("null or empty argument");
     return FAME_ERR_BAD_INPUT;
@@ -844,12 +850,13 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     s.ls_maxit = p.ls_maxit;
     s.mixed = p.precision == FAME_MIXED;
     s.vec = p.want_vectors ? 1 : 0;
+    s.enorm = resabs_out ? 1 : 0;
     s.es_tol = p.es_tol;
     s.ls_tol = p.ls_tol;
     s.inner_tol = p.inner_tol > 0 ? p.inner_tol : 2e-6;  // two FP64 refinement steps reach 1e-12
     s.inner_maxit = p.inner_maxit > 0 ? p.inner_maxit : 200;
     const bool graph = p.use_graph != 0;
-    ensure_workspace(c, s.nslots, s.nstep, s.nwant, s.mixed, s.vec);
+    ensure_workspace(c, s.nslots, s.nstep, s.nwant, s.mixed, s.vec || s.enorm);
     const std::string key = cfg_key(s, graph);
     auto it = c->progs.find(key);
     Program* P = nullptr;
@@ -866,7 +873,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     }
     const long N = c->g.N;
     std::vector<Slot> hs(s.nslots);
-    std::vector<double> theta((size_t)s.nslots * s.nstep), stats((size_t)s.nslots * s.nwant * 4);
+    std::vector<double> theta((size_t)s.nslots * s.nstep), stats((size_t)s.nslots * s.nwant * 5);
     std::vector<LzState> lz(s.nslots);
     std::vector<int> prof(3 * s.nslots), status(s.nslots);
     for (int b0 = 0; b0 < nk; b0 += s.nslots) {
@@ -913,7 +920,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
       for (int q = 0; q < nb; q++) {
         const int kk = b0 + q;
         const bool gamma = hs[q].Nd == N - 1;
-        std::vector<double> f(s.nwant), rr(s.nwant), re(s.nwant);
+        std::vector<double> f(s.nwant), rr(s.nwant), re(s.nwant), ra(s.nwant);
         for (int i = 0; i < s.nwant; i++) {
           const double th = theta[(size_t)q * s.nstep + i];
           f[i] = sqrt(1.0 / th);
@@ -922,23 +929,30 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
           rr[i] = sqrt(st[0]) / (lam * sqrt(st[1]));
           const double rho = st[2] / st[3];
           re[i] = fabs(lam - rho) / rho;
+          // ||C^H C E - w^2 B E|| = sqrt(st[0] / N) for E = B^-1 Q_r Sigma y (Q_r carries
+          // the 1/N of the unnormalised inverse DFT, so ||Q_r z|| = ||z|| / sqrt(N)); the
+          // reference restores s E with s = ||E|| (FAME_Fast_Algorithms_Isotropic.cu:119-121)
+          ra[i] = s.enorm ? stats[(size_t)s.nslots * s.nwant * 4 + (size_t)q * s.nwant + i] * sqrt(st[0] / N) : 0.0;
         }
         // Gamma patch: bands shift up by two, w0 = w1 = 0 (FAME_Fast_Algorithms_Isotropic.cu:61-79)
-        std::vector<double> fo(f), ro(rr), eo(re);
+        std::vector<double> fo(f), ro(rr), eo(re), ao(ra);
         if (gamma) {
           for (int i = s.nwant - 1; i >= 2; i--) {
             fo[i] = f[i - 2];
             ro[i] = rr[i - 2];
             eo[i] = re[i - 2];
+            ao[i] = ra[i - 2];
           }
           fo[0] = fo[1] = 0.0;
           ro[0] = ro[1] = 0.0;
           eo[0] = eo[1] = 0.0;
+          ao[0] = ao[1] = 0.0;  // constant E: C E = 0
         }
         for (int i = 0; i < s.nwant; i++) {
           freq_out[(size_t)kk * s.nwant + i] = fo[i];
           if (relres_out) relres_out[(size_t)kk * s.nwant + i] = ro[i];
           if (relerr_out) relerr_out[(size_t)kk * s.nwant + i] = eo[i];
+          if (resabs_out) resabs_out[(size_t)kk * s.nwant + i] = ao[i];
         }
         if (counters) {
           fame_kcounters& kc = counters[kk];

@@ -74,7 +74,7 @@ def load():
     lib.fame_ctx_destroy.restype = None
     lib.fame_set_eps.argtypes = [P, D]
     lib.fame_set_material.argtypes = [P, C.POINTER(C.c_int), C.c_int, D, C.c_double]
-    lib.fame_solve_kpoints.argtypes = [P, D, C.c_int, C.POINTER(SolverParams), D, D, D, D, C.POINTER(KCounters)]
+    lib.fame_solve_kpoints.argtypes = [P, D, C.c_int, C.POINTER(SolverParams), D, D, D, D, D, C.POINTER(KCounters)]
     lib.fame_apply.argtypes = [P, C.c_int, D, P, P, C.c_int, C.POINTER(SolverParams), C.POINTER(C.c_int)]
     lib.fame_adjoint.argtypes = [P, D, D, C.c_int, C.c_int, D]
     lib.fame_ctx_sizes.argtypes = [P, C.POINTER(C.c_longlong)]
@@ -158,8 +158,9 @@ class Context:
         _check(load().fame_set_material(self._h, b.ctypes.data_as(C.POINTER(C.c_int)), int(material_num),
                                         _dptr(e), float(eps_out)))
 
-    def solve(self, kpoints, params=None, **kw):
-        """Returns dict(freq, relres, relerr, counters[, evec]) for kpoints (nk, 3)."""
+    def solve(self, kpoints, params=None, resabs=False, **kw):
+        """Returns dict(freq, relres, relerr, counters[, resabs][, evec]) for kpoints (nk, 3).
+        resabs: also the residual norm of E scaled as the reference restores it."""
         p = params or solver_params(**kw)
         k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
         nk = k.shape[0]
@@ -168,13 +169,17 @@ class Context:
         re = np.zeros((nk, p.nwant))
         ev = np.zeros((nk, p.nwant, 3 * self.N), dtype=np.complex128) if p.want_vectors else None
         cnt = (KCounters * nk)()
+        ra = np.zeros((nk, p.nwant)) if resabs else None
         rc = load().fame_solve_kpoints(self._h, _dptr(k), nk, C.byref(p), _dptr(freq), _dptr(rr), _dptr(re),
+                                       _dptr(ra) if ra is not None else None,
                                        ev.ctypes.data_as(C.POINTER(C.c_double)) if ev is not None else None, cnt)
         out = dict(freq=freq, relres=rr, relerr=re, rc=rc,
                    counters=[dict(ls_iter=c.ls_iter, es_iter=c.es_iter, restarts=c.restarts, status=c.status,
                                   Nd=c.Nd, refine=c.refine) for c in cnt])
         if ev is not None:
             out["evec"] = ev
+        if ra is not None:
+            out["resabs"] = ra
         if rc not in (OK, ERR_NO_CONVERGENCE):
             _check(rc)
         return out

@@ -106,13 +106,17 @@ int fame_set_material(fame_ctx* ctx, const int* binout, int material_num, const 
  *                         + Lanczos_Isotropic.cu:88, Gamma patch :61-79);
  *   relres_out nk*nwant   ||C^H C E - w^2 B E|| / (w^2 ||B E||) evaluated in FP64, or NULL;
  *   relerr_out nk*nwant   |w^2 - rho| / rho with rho the FP64 Rayleigh quotient, or NULL;
+ *   resabs_out nk*nwant   ||C^H C E - w^2 B E|| for E scaled as the reference restores it
+ *                         (FAME_Fast_Algorithms_Isotropic.cu:119-121), the quantity its
+ *                         Check_Residual tests against 1e-10 (FAME_Main_Code.cu:383-421),
+ *                         or NULL (non-NULL adds one Q_r apply per band);
  *   evec_out   nk*nwant*3N complex128 (params->want_vectors), or NULL;
  *   counters   nk entries, or NULL.
  * Replaces FAME_Fast_Algorithms_Driver (FAME_Main/FAME_Main_Code.cu:142-171) over
  * the k-loop of FAME_Main_Code (:79-133). */
 int fame_solve_kpoints(fame_ctx* ctx, const double* k_xyz, int nk, const fame_solver_params* params,
-                       double* freq_out, double* relres_out, double* relerr_out, double* evec_out,
-                       fame_kcounters* counters);
+                       double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
+                       double* evec_out, fame_kcounters* counters);
 
 /* Apply one operator at one k-point on device buffers (complex, interleaved):
  * in/out are device pointers of length given in the FAME_OP_* comments.

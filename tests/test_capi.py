@@ -33,7 +33,7 @@ def test_null_arguments_are_rejected():
     lib = fb.load()
     assert lib.fame_ctx_create(0, None, None) == fb.ERR_BAD_INPUT
     assert lib.fame_set_eps(None, None) == fb.ERR_BAD_INPUT
-    assert lib.fame_solve_kpoints(None, None, 0, None, None, None, None, None, None) == fb.ERR_BAD_INPUT
+    assert lib.fame_solve_kpoints(None, None, 0, None, None, None, None, None, None, None) == fb.ERR_BAD_INPUT
     assert b"null" in lib.fame_last_error()
 
 
