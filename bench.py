@@ -111,17 +111,21 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def dist_init():
+def dist_init(backend="nccl", timeout_s=600):
+    """One process per GPU (torchrun sets RANK / LOCAL_RANK / WORLD_SIZE / MASTER_*).
+    The process-group timeout bounds every collective, so ranks that wait for a
+    rank that has failed end with an error instead of hanging."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws == 1:
         return 0, 1, 0, None
+    import datetime
     import torch
     import torch.distributed as dist
     rank = int(os.environ["RANK"])
     local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
-    import datetime
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return rank, ws, local, dist
 
 
@@ -129,7 +133,8 @@ def max_over_ranks(x, dist):
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
