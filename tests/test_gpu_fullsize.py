@@ -72,3 +72,26 @@ def test_general_lattices_full_size(name):
     assert mx["rc"] == fb.OK
     assert _relerr(mx["freq"], fr) < 1e-6
     assert np.all(mx["relerr"] < 1e-6)
+
+
+def test_batched_band_path_in_one_graph():
+    """BCC 48x45x39: 60 k-points along Gamma-H-N-Gamma-P (15 per segment, segment
+    end excluded, built from the reference's vertex list), 12 bands, mixed precision,
+    all 60 k-points as one batch in one CUDA graph.  The Gamma, H and N points match
+    the reference's frequencies; three interior k-points solved one at a time match
+    the batched result (the slots of a batch do not interact)."""
+    par = load_pre("bcc48")
+    v = par["kpoints"]  # Gamma, H, N, Gamma, P, ... (the reference's path GHNGPH|PN)
+    seg = [(v[0], v[1]), (v[1], v[2]), (v[2], v[3]), (v[3], v[4])]
+    k = np.array([a + (b - a) * (i / 15.0) for a, b in seg for i in range(15)])
+    _, fr, _, tol = _ref("bcc48")
+    ctx = _ctx(par)
+    out = ctx.solve(k, nwant=12, precision=fb.MIXED, batch=60, use_graph=1, **_tols(tol))
+    assert out["rc"] == fb.OK
+    assert np.all(out["relerr"] < 1e-6)
+    # Gamma (0 and 45), H (15), N (30) against the reference's k 0, 1, 2
+    for i, r in ((0, 0), (15, 1), (30, 2), (45, 0)):
+        assert _relerr(out["freq"][i:i + 1], fr[r:r + 1]) < 1e-6, i
+    sub = [7, 22, 52]
+    one = ctx.solve(k[sub], nwant=12, precision=fb.MIXED, batch=1, use_graph=1, **_tols(tol))
+    assert np.max(np.abs(one["freq"] - out["freq"][sub]) / out["freq"][sub]) < 1e-10
