@@ -686,12 +686,29 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
   }
 }
 
-static int choose_batch(const fame_ctx* c, int nk, const fame_solver_params* p) {
+// Device bytes of one slot's workspace (the per-slot buffers of ensure_workspace).
+static double slot_bytes(const fame_ctx* c, int nstep, int nwant, bool mixed, bool vec) {
+  const double N = c->g.N, M = 2.0 * N, z = 16.0;
+  double b = (nstep + 1 + nwant + 1) * M * z   // Lanczos basis U
+             + 2 * M * z + 3 * N * z           // r64, x64, T64
+             + 2 * nwant * M * z + nwant * 3 * N * z  // EV, AV, Tb
+             + 2 * M * z;                      // p64, Ap64
+  if (mixed) b += M * z + 4 * M * 8 + 3 * N * 8;  // b64, r32, x32, p32, Ap32, T32
+  if (vec) b += nwant * 3 * N * z;               // E
+  return b;
+}
+
+// k-points per batch.  The stage kernels of one k-point do not fill the GPU (a 96^3
+// plane stage is 96 three-CTA clusters, slightly more than fit at once), so several
+// k-points per launch pay: as many as 60% of the free device memory holds, at most 64.
+static int choose_batch(const fame_ctx* c, int nk, const fame_solver_params* p, bool vec) {
   if (p->batch > 0) return std::min(p->batch, nk);
-  // keep one batch's CG working set (about 88 N bytes in FP32) inside the 126 MB L2
-  const double ws = 100.0 * c->g.N;
-  int b = (int)std::max(1.0, floor(90e6 / ws));
-  return std::max(1, std::min({b, nk, 32}));
+  size_t free_b = 0, total_b = 0;
+  FAME_CK(cudaMemGetInfo(&free_b, &total_b));
+  const bool mixed = p->precision == FAME_MIXED;
+  const double per = slot_bytes(c, p->nstep, p->nwant, mixed, vec);
+  const int b = (int)std::max(1.0, floor(0.6 * (double)free_b / per));
+  return std::max(1, std::min({b, nk, 64}));
 }
 
 }  // namespace fame
@@ -843,7 +860,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
   try {
     FAME_CK(cudaSetDevice(c->device));
     SolveCfg s;
-    s.nslots = choose_batch(c, nk, &p);
+    s.nslots = choose_batch(c, nk, &p, p.want_vectors || resabs_out);
     s.nstep = p.nstep;
     s.nwant = p.nwant;
     s.es_maxit = p.es_maxit;
@@ -1150,8 +1167,10 @@ int fame_launch_count(fame_ctx* c, unsigned long long* out) {
   return FAME_OK;
 }
 
-int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, double* ms_out, double* stage_ms) {
-  if (!c || !k || !ms_out || reps < 1 || (precision != FAME_FP64 && precision != FAME_MIXED)) {
+int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, int nbatch, double* ms_out,
+                   double* stage_ms) {
+  if (!c || !k || !ms_out || reps < 1 || nbatch < 1 || nbatch > 64 ||
+      (precision != FAME_FP64 && precision != FAME_MIXED)) {
     set_err("bad argument");
     return FAME_ERR_BAD_INPUT;
   }
@@ -1161,7 +1180,7 @@ int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, double
   }
   try {
     FAME_CK(cudaSetDevice(c->device));
-    ensure_workspace(c, 1, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), precision == FAME_MIXED,
+    ensure_workspace(c, nbatch, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), precision == FAME_MIXED,
                      c->cap_vec);
     Slot sl;
     memset(&sl, 0, sizeof(sl));
@@ -1169,13 +1188,14 @@ int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, double
     sl.Nd = reduced_size(c->lat, k);
     sl.off = c->g.N - sl.Nd;
     sl.active = 1;
-    FAME_CK(cudaMemcpyAsync(c->slots.p, &sl, sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
+    std::vector<Slot> hs(nbatch, sl);  // the same k-point in every slot of the batch
+    FAME_CK(cudaMemcpyAsync(c->slots.p, hs.data(), nbatch * sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
     Program P(c->stream, false, c->hflag, 1);
-    Ops o{c, P, 1};
+    Ops o{c, P, nbatch};
     const Geom& g = c->g;
     const long M = 2L * g.N, F = 3L * g.N;
     const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
-    P.launch(k_tables, dim3((tmax + 255) / 256, 1), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
+    P.launch(k_tables, dim3((tmax + 255) / 256, nbatch), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
              (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
     DBuf<unsigned char> flush;
     const size_t fl = 256ull << 20;
@@ -1185,9 +1205,9 @@ int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, double
     double tot[3] = {0, 0, 0};
     // input: r64 / r32 hold arbitrary finite data after a memset
     if (precision == FAME_FP64)
-      FAME_CK(cudaMemsetAsync(c->r64.p, 0, M * sizeof(double2), c->stream));
+      FAME_CK(cudaMemsetAsync(c->r64.p, 0, nbatch * M * sizeof(double2), c->stream));
     else
-      FAME_CK(cudaMemsetAsync(c->r32.p, 0, M * sizeof(float2), c->stream));
+      FAME_CK(cudaMemsetAsync(c->r32.p, 0, nbatch * M * sizeof(float2), c->stream));
     for (int it = 0; it < reps + 1; it++) {
       FAME_CK(cudaMemsetAsync(flush.p, it & 0xff, fl, c->stream));
       FAME_CK(cudaEventRecord(ev[0], c->stream));

@@ -81,7 +81,7 @@ def load():
     lib.fame_ctx_stream.argtypes = [P]
     lib.fame_ctx_stream.restype = C.c_void_p
     lib.fame_launch_count.argtypes = [P, C.POINTER(C.c_ulonglong)]
-    lib.fame_bench_qbq.argtypes = [P, D, C.c_int, C.c_int, D, D]
+    lib.fame_bench_qbq.argtypes = [P, D, C.c_int, C.c_int, C.c_int, D, D]
     lib.fame_qbq_static.argtypes = [C.POINTER(Lattice), D, P, P, P, P]
     lib.fame_last_error.restype = C.c_char_p
     lib.fame_version.restype = C.c_char_p
@@ -203,12 +203,14 @@ class Context:
         _check(load().fame_launch_count(self._h, C.byref(n)))
         return n.value
 
-    def bench_qbq(self, k, precision=MIXED, reps=20):
-        """Mean device ms of one L2-cold Q_r^* B^-1 Q_r apply and of its 3 stages."""
+    def bench_qbq(self, k, precision=MIXED, reps=20, nbatch=1):
+        """Mean device ms of one L2-cold Q_r^* B^-1 Q_r apply to a batch of nbatch
+        vectors, and of its 3 stages."""
         kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
         ms = C.c_double()
         st = np.zeros(3)
-        _check(load().fame_bench_qbq(self._h, _dptr(kk), int(precision), int(reps), C.byref(ms), _dptr(st)))
+        _check(load().fame_bench_qbq(self._h, _dptr(kk), int(precision), int(reps), int(nbatch), C.byref(ms),
+                                     _dptr(st)))
         return ms.value, st
 
     def adjoint(self, freq, evec):

@@ -69,7 +69,7 @@ typedef struct {
   int ls_maxit;     /* LS.maxit */
   double ls_tol;    /* LS.tol: absolute ||r|| of the inner solve */
   int precision;    /* FAME_FP64 or FAME_MIXED */
-  int batch;        /* k-points in flight per launch (0 = automatic) */
+  int batch;        /* k-points per launch (0 = automatic: what 60% of free device memory holds, <= 64) */
   int use_graph;    /* 1 = run each batch as one CUDA graph (default), 0 = host-driven loop */
   double inner_tol; /* FAME_MIXED: relative tolerance of each FP32 inner solve (0 = 2e-6) */
   int inner_maxit;  /* FAME_MIXED: products per FP32 inner solve (0 = 200) */
@@ -143,12 +143,13 @@ void* fame_ctx_stream(fame_ctx* ctx);
 int fame_launch_count(fame_ctx* ctx, unsigned long long* count_out);
 
 /* Operator benchmark: `reps` applications of Q_r^* B^-1 Q_r at wave vector k in
- * FP64 (precision FAME_FP64) or FP32 (FAME_MIXED), each preceded by an L2 flush
- * (a 256 MiB device write) outside the timed span; CUDA events on the context
- * stream.  stage_ms_out[3] (optional) receives the mean device time of the plane
- * inverse stage, the pencil stage and the plane forward stage; ms_out the mean of
- * their sum. */
-int fame_bench_qbq(fame_ctx* ctx, const double* k, int precision, int reps, double* ms_out,
+ * FP64 (precision FAME_FP64) or FP32 (FAME_MIXED) to a batch of `nbatch` vectors
+ * (1..64, the k-point repeated in every slot, as the solver batches k-points), each
+ * preceded by an L2 flush (a 256 MiB device write) outside the timed span; CUDA
+ * events on the context stream.  stage_ms_out[3] (optional) receives the mean
+ * device time of the plane inverse stage, the pencil stage and the plane forward
+ * stage over the whole batch; ms_out the mean of their sum. */
+int fame_bench_qbq(fame_ctx* ctx, const double* k, int precision, int reps, int nbatch, double* ms_out,
                    double* stage_ms_out);
 
 /* Grid size N and maximum reduced size 2N of the context, for buffer sizing. */

@@ -189,6 +189,10 @@ static int mode_solve(const char* out, const char* kfile, const char* epsfile,
   for (int i : which) {
     if (i < 0 || i >= nk) die("k index out of range");
     c.Profile.idx = i;
+    // the reference accumulates its counters per k index: a k solved again in this
+    // run (bench warm-up and timed steps) reports its own counts
+    c.Profile.ls_iter[i] = 0;
+    c.Profile.es_iter[i] = 0;
     double wv[3] = {c.k[3 * i], c.k[3 * i + 1], c.k[3 * i + 2]};
     LAMBDAS L;
     LAMBDAS_CUDA Lc;
