@@ -351,6 +351,36 @@ def run_qbq(args):
     ctx.close()
 
 
+def run_locate(args):
+    """The material map Binout of the hexagonal 128x107x92 workload: fame_material_locate
+    (host in, host out) against the reference's CPU preprocessing, whose time is
+    dominated by FAME_Material_Locate_Index (fame_ref_harness pre, the same inputs)."""
+    import fame_b200 as fb
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from fixtures import load_pre
+    par = load_pre("hex128")
+    call = lambda: fb.material_locate(par["grid"], par["mesh_len"], par["lattice_vec_a"], par["Omega"],
+                                      par["Permutation"], par["material"])
+    for _ in range(max(1, args.warmup)):
+        b = call()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        b = call()
+    t = (time.perf_counter() - t0) / max(1, args.steps)
+    line = {"mode": "locate", "workload": "hex c/a=1.2, 128x107x92, 2 cylinders r=0.3", "gpu_s": round(t, 5),
+            "bit_exact": bool(np.array_equal(b, par["binout"]))}
+    harness = os.path.join(ROOT, "oracle", "_ref", "fame_ref_harness")
+    if os.path.exists(harness):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref_inputs as ri
+        with tempfile.TemporaryDirectory() as d:
+            ri.make_workdir("hex128", d)
+            t0 = time.perf_counter()
+            subprocess.run([harness, "pre", d, os.path.join(d, "pre.bin")], check=True, stdout=subprocess.DEVNULL)
+            line["reference_preprocessing_s"] = round(time.perf_counter() - t0, 3)
+    print(json.dumps(line), flush=True)
+
+
 def edge_eps(W, N):
     """B (3N) from the material map with FAME_Matrix_B_Isotropic's last-wins rule."""
     B = np.full(3 * N, W["eps_out"])
@@ -425,7 +455,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "qbq"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "qbq", "locate"],
                     help="qbq: only time Q_r^* B^-1 Q_r applies at 96^3 (--steps applies; for kernel profiles)")
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven loops instead of the CUDA graph (launch lists under ncu)")
@@ -438,6 +468,8 @@ def main():
         return run_reference(args)
     if args.mode == "qbq":
         return run_qbq(args)
+    if args.mode == "locate":
+        return run_locate(args)
     return run_ours(args)
 
 

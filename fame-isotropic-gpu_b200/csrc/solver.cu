@@ -37,6 +37,7 @@ unsigned long long launches_ops_f64_simple_rare();
 unsigned long long launches_ops_f64_general_rare();
 unsigned long long launches_ops_stat96_f32();
 unsigned long long launches_ops_stat96_f64();
+unsigned long long launches_material_locate();
 FAME_DEFINE_LAUNCH_GETTER(launches_solver)
 
 static thread_local std::string g_err;
@@ -1159,7 +1160,7 @@ int fame_launch_count(fame_ctx* c, unsigned long long* out) {
     *out = launches_solver() + launches_ops_f32_simple() + launches_ops_f32_general() + launches_ops_f64_simple() +
            launches_ops_f64_general() + launches_ops_f32_simple_rare() + launches_ops_f32_general_rare() +
            launches_ops_f64_simple_rare() + launches_ops_f64_general_rare() + launches_ops_stat96_f32() +
-           launches_ops_stat96_f64();
+           launches_ops_stat96_f64() + launches_material_locate();
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;

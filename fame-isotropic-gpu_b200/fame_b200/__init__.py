@@ -29,7 +29,7 @@ OP_QR, OP_QRS, OP_QBQ, OP_PR, OP_PRS, OP_INVAR = range(6)
 # every symbol declared in include/fame_b200.h
 EXPORTS = ("fame_ctx_create", "fame_ctx_destroy", "fame_set_eps", "fame_set_material", "fame_solve_kpoints",
            "fame_apply", "fame_adjoint", "fame_ctx_sizes", "fame_last_error", "fame_version", "fame_ctx_stream",
-           "fame_launch_count", "fame_bench_qbq", "fame_qbq_static")
+           "fame_launch_count", "fame_bench_qbq", "fame_qbq_static", "fame_material_locate")
 QBQ_STATIC_SCRATCH_BYTES = 4 << 20  # FAME_QBQ_STATIC_SCRATCH_BYTES
 
 
@@ -49,6 +49,18 @@ class SolverParams(C.Structure):
                 ("ls_maxit", C.c_int), ("ls_tol", C.c_double), ("precision", C.c_int), ("batch", C.c_int),
                 ("use_graph", C.c_int), ("inner_tol", C.c_double), ("inner_maxit", C.c_int),
                 ("want_vectors", C.c_int)]
+
+
+class LocateGeometry(C.Structure):
+    _fields_ = [("grid", C.c_int * 3), ("mesh_len", C.c_double * 3), ("lattice_vec_a", C.c_double * 9),
+                ("Omega", C.c_double * 9), ("permutation", C.c_int * 3)]
+
+
+class MaterialShapes(C.Structure):
+    _fields_ = [("material_num", C.c_int), ("sphere_num", C.POINTER(C.c_int)),
+                ("sphere_centers", C.POINTER(C.c_double)), ("sphere_radius", C.POINTER(C.c_double)),
+                ("cylinder_num", C.POINTER(C.c_int)), ("cylinder_top_centers", C.POINTER(C.c_double)),
+                ("cylinder_bot_centers", C.POINTER(C.c_double)), ("cylinder_radius", C.POINTER(C.c_double))]
 
 
 class KCounters(C.Structure):
@@ -83,10 +95,13 @@ def load():
     lib.fame_launch_count.argtypes = [P, C.POINTER(C.c_ulonglong)]
     lib.fame_bench_qbq.argtypes = [P, D, C.c_int, C.c_int, C.c_int, D, D]
     lib.fame_qbq_static.argtypes = [C.POINTER(Lattice), D, P, P, P, P]
+    lib.fame_material_locate.argtypes = [C.c_int, C.POINTER(LocateGeometry), C.POINTER(MaterialShapes),
+                                         C.POINTER(C.c_int)]
     lib.fame_last_error.restype = C.c_char_p
     lib.fame_version.restype = C.c_char_p
     for fn in ("fame_ctx_create", "fame_set_eps", "fame_set_material", "fame_solve_kpoints", "fame_apply",
-               "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq", "fame_qbq_static"):
+               "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq", "fame_qbq_static",
+               "fame_material_locate"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib
@@ -221,6 +236,38 @@ class Context:
         g = np.zeros((nw, self.N))
         _check(load().fame_adjoint(self._h, _dptr(f), e.ctypes.data_as(C.POINTER(C.c_double)), nw, 1, _dptr(g)))
         return g
+
+
+def material_locate(grid, mesh_len, lattice_vec_a, Omega, permutation, material, device=0):
+    """Binout (int32, 3 * material_num * N) on the GPU through fame_material_locate.
+    material: dict with material_num, sphere_num, sphere_centers, sphere_radius,
+    cylinder_num, cylinder_top_centers, cylinder_bot_centers, cylinder_radius."""
+    g = LocateGeometry()
+    g.grid[:] = [int(v) for v in grid]
+    g.mesh_len[:] = [float(v) for v in mesh_len]
+    g.lattice_vec_a[:] = [float(v) for v in lattice_vec_a]
+    g.Omega[:] = [float(v) for v in Omega]
+    g.permutation[:] = [int(v) for v in permutation]
+    keep = []
+
+    def arr(v, t):
+        a = np.ascontiguousarray(np.asarray(v, dtype=t).reshape(-1))
+        keep.append(a)
+        ct = C.c_int if t == np.int32 else C.c_double
+        return a.ctypes.data_as(C.POINTER(ct)) if a.size else None
+
+    m = MaterialShapes()
+    m.material_num = int(material["material_num"])
+    m.sphere_num = arr(material["sphere_num"], np.int32)
+    m.sphere_centers = arr(material["sphere_centers"], np.float64)
+    m.sphere_radius = arr(material["sphere_radius"], np.float64)
+    m.cylinder_num = arr(material["cylinder_num"], np.int32)
+    m.cylinder_top_centers = arr(material["cylinder_top_centers"], np.float64)
+    m.cylinder_bot_centers = arr(material["cylinder_bot_centers"], np.float64)
+    m.cylinder_radius = arr(material["cylinder_radius"], np.float64)
+    out = np.zeros(3 * m.material_num * int(np.prod(grid)), dtype=np.int32)
+    _check(load().fame_material_locate(int(device), C.byref(g), C.byref(m), out.ctypes.data_as(C.POINTER(C.c_int))))
+    return out
 
 
 def qbq_static(lattice, k, inv_b, x, y, stream=0):

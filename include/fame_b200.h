@@ -155,6 +155,39 @@ int fame_bench_qbq(fame_ctx* ctx, const double* k, int precision, int reps, int 
 /* Grid size N and maximum reduced size 2N of the context, for buffer sizing. */
 int fame_ctx_sizes(const fame_ctx* ctx, long long* N_out);
 
+/* Geometry of the material map (the reference's PAR fields, include/FAME_Internal_Common.h:64-99,
+ * 124-131): grid = Par.mesh.grid_nums, mesh_len = Par.mesh.mesh_len, lattice_vec_a and Omega
+ * = Par.lattice.lattice_vec_a / Omega (column major), permutation = Par.lattice.Permutation. */
+typedef struct {
+  int grid[3];
+  double mesh_len[3];
+  double lattice_vec_a[9];
+  double Omega[9];
+  int permutation[3];
+} fame_locate_geometry;
+
+/* Shapes of each material (Par.material, include/FAME_Internal_Common.h:93-110): material m
+ * owns sphere_num[m] spheres and cylinder_num[m] cylinders, listed material by material;
+ * centres are fractional coordinates of the original lattice (3 doubles each). */
+typedef struct {
+  int material_num;
+  const int* sphere_num;
+  const double* sphere_centers;
+  const double* sphere_radius;
+  const int* cylinder_num;
+  const double* cylinder_top_centers;
+  const double* cylinder_bot_centers;
+  const double* cylinder_radius;
+} fame_material_shapes;
+
+/* The material index map Binout (host, 3 * material_num * N ints: x-, y-, z-edge blocks, each
+ * material_num blocks of N, 1 where the edge point lies in that material, the first material
+ * that contains it) computed on `device`, bit-exact with the reference's CPU
+ * FAME_Material_Locate_Index (FAME_Preprocessing/FAME_Material_Locate_Index.cpp:6-113,
+ * FAME_Material_Handle.cpp:4-87).  Feed it to fame_set_material. */
+int fame_material_locate(int device, const fame_locate_geometry* geo, const fame_material_shapes* mat,
+                         int* binout);
+
 /* Bytes of the fixed device scratch array behind fame_qbq_static. */
 #define FAME_QBQ_STATIC_SCRATCH_BYTES (4u << 20)
 
