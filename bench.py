@@ -4,22 +4,23 @@
 Workload: simple cubic lattice a=1, grid 96^3, one dielectric sphere (r=0.25a,
 eps=13) in eps=1, 10 bands, Lanczos restart dimension 40, Lanczos and CG
 tolerances 1e-12 (the reference's defaults; relative residual of every band
-checked <= 1e-6), the
-reference's default band path GXMGRX|MR with part_num=4 (20 k-points).  The k
+checked <= 1e-6), the reference's default band path GXMGRX|MR with part_num=4
+(20 k-points).  The k
 path and the material map are the reference preprocessing outputs committed in
 tests/golden/sc96_pre.npz (synthetic crystal; no dataset involved).
 
 One step = one full solve of the 20-k path through the device-resident solver
-(inputs already in HBM).  The working set of one batch is larger than L2 only in
-FP64; each step runs >1000 CG iterations, so L2 state between steps is irrelevant
-(config records "l2": "inputs exceed L2 per step").
+(inputs already in HBM), all 20 k-points as one batch in one CUDA graph.  The
+batch's working set (about 55 GB) is far larger than L2 and each step runs >1000
+CG iterations, so L2 state between steps is irrelevant (config records "l2").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision mixed|fp64] [--no-fp64] [--no-cpu-baseline]
+                  [--precision mixed|fp64] [--batch B] [--no-fp64] [--no-cpu-baseline]
+                  [--mode solve|qbq|locate] [--nk K] [--tol T] [--no-graph]
 
 --impl reference runs the reference's own FP64 CUDA build (oracle/_ref, compiled
-from the reference sources) through its own FAME_Fast_Algorithms_Driver on a
-bounded sample of the same path (4 k-points per step).
+from the reference sources) through its own FAME_Fast_Algorithms_Driver; each
+timed step is the whole 20-point path, one k-point at a time.
 """
 from __future__ import annotations
 
