@@ -446,14 +446,11 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
     c->p32.ensure((size_t)nslots * M);
     c->Ap32.ensure((size_t)nslots * M);
     c->T32.ensure((size_t)nslots * 3 * N);
-  } else {
-    c->p64.ensure((size_t)nslots * M);
-    c->Ap64.ensure((size_t)nslots * M);
   }
-  if (mixed && !c->p64.p) {
-    c->p64.ensure((size_t)nslots * M);
-    c->Ap64.ensure((size_t)nslots * M);
-  }
+  // FP64 CG vectors: every context may run FP64 solves and A_r^-1 applies, whatever
+  // precision it started with, so they grow with the slot count in both modes
+  c->p64.ensure((size_t)nslots * M);
+  c->Ap64.ensure((size_t)nslots * M);
   if (vec) c->E.ensure((size_t)nslots * nwant * 3 * N);
   c->cap_slots = nslots;
   c->cap_nstep = nstep;

@@ -100,3 +100,18 @@ def test_gamma_point_patch():
     assert out["freq"][0, 0] == 0 and out["freq"][0, 1] == 0
     v = 1.0 / np.sqrt(3 * par["N"])
     assert np.allclose(out["evec"][0, 0], v) and np.allclose(out["evec"][0, 1], v)
+
+
+def test_precision_and_batch_changes_on_one_context():
+    """One context grows its batch in mixed precision (1 then 3 k-points) and then
+    solves the same 3 k-points in FP64: every workspace buffer follows the largest
+    batch seen, whichever precision asked for it."""
+    par = load_pre("sc16")
+    k, fr, _ = _ref("sc16")
+    ctx = _ctx(par)
+    ctx.solve(k[:1], nwant=10, precision=fb.MIXED, **TOL)
+    mx = ctx.solve(k[1:4], nwant=10, precision=fb.MIXED, **TOL)
+    f64 = ctx.solve(k[1:4], nwant=10, precision=fb.FP64, **TOL)
+    assert mx["rc"] == fb.OK and f64["rc"] == fb.OK
+    assert _relerr(mx["freq"], fr[1:4]) < 1e-6
+    assert _relerr(f64["freq"], fr[1:4]) < 1e-8
