@@ -15,8 +15,9 @@
 // of its butterflies, the block synchronises, then every thread writes, so the
 // transform runs in place in one shared buffer.  Radices 2,3,4,5,7,8 (and odd
 // 11, 13 through the symmetric-pair DFT) use butterflies; any other factor (a
-// large prime such as 23 or 107) uses an output-stationary DFT pass where each
-// thread forms its outputs as length-R sums.
+// large prime such as 23 or 107) uses a register-blocked symmetric-pair DFT pass
+// (prime_pass), or an output-stationary pass where each thread forms its outputs
+// as length-R sums when a line needs more threads than the block has.
 #pragma once
 #include "fame_common.cuh"
 
@@ -329,6 +330,158 @@ __device__ __forceinline__ void generic_pass(cplx<R>* buf, int n, int r, int Ns,
   }
 }
 
+// Odd radix r (a prime >= 17) through symmetric pairs, in two phases.
+// Phase A, over all lines at once: butterfly j's inputs a_s = x[j + s*nb] take the
+// Stockham twiddle w^(s*k*stw) (k = j mod Ns) and are replaced in place by
+// P_s = a_s + a_{r-s} at s and Q_s = a_s - a_{r-s} at r - s (1 <= s <= H).
+// Phase B, in rounds of complete lines:
+//   X_u = a_0 + sum_s cos(2 pi us/r) P_s -/+ i sum_s sin(2 pi us/r) Q_s,
+//   X_{r-u} the same with the sign of the second sum flipped (u = 0..H).
+// A thread owns one butterfly j, MU consecutive u and up to ML lines (Gt apart), so
+// each loaded P_s, Q_s feeds MU outputs and each cos/sin feeds ML lines: 4*MU*ML
+// FMAs per 2*ML + MU shared-memory loads.  cos/sin come from the axis table,
+// tw[(us mod r)*nb] = e^{-2 pi i us/r}.  Returns false (nothing done) when one
+// line's MU-groups exceed the block; the caller then takes the output-stationary
+// pass.
+template <typename R, int MU, int ML>
+__device__ __forceinline__ bool prime_pass(cplx<R>* buf, int n, int r, int Ns, LineSet L, const cplx<R>* tw,
+                                           bool inv) {
+  const int T = blockDim.x;
+  const int nb = n / r;
+  const int stw = n / (Ns * r);
+  const int H = (r - 1) / 2;
+  const int ug = (H + MU) / MU;  // groups of MU covering u = 0..H
+  const int cells = nb * ug;
+  if (cells > T) return false;
+  // phase A
+  {
+    const Div dl(L.nl), dnb(nb), dns(Ns);
+    const int tot = L.nl * nb * H;
+    for (int i = threadIdx.x; i < tot; i += T) {
+      const int q = (int)dl.q(i);
+      const int l = i - q * L.nl;
+      const int sq = (int)dnb.q(q);
+      const int j = q - sq * nb;
+      const int s = sq + 1;
+      const int k = j - (int)dns.q(j) * Ns;
+      cplx<R>* base = buf + l * L.ls;
+      cplx<R>* pa = base + (j + s * nb) * L.es;
+      cplx<R>* pb = base + (j + (r - s) * nb) * L.es;
+      cplx<R> a = *pa, b = *pb;
+      if (k > 0) {
+        cplx<R> wa = tw[s * k * stw], wb = tw[(r - s) * k * stw];
+        if (inv) {
+          wa.y = -wa.y;
+          wb.y = -wb.y;
+        }
+        a = cmul(a, wa);
+        b = cmul(b, wb);
+      }
+      *pa = cadd(a, b);
+      *pb = csub(a, b);
+    }
+  }
+  __syncthreads();
+  // phase B
+  const int Gt = min(L.nl, T / cells);
+  const int t = threadIdx.x;
+  const int cell = t / Gt;
+  const int lt = t - cell * Gt;
+  const bool live = cell < cells;
+  const int ugi = cell / nb;
+  const int j = cell - ugi * nb;
+  const int u0 = ugi * MU;
+  const int jb = j / Ns;
+  const int k = j - jb * Ns;
+  const int ostep = Ns * L.es;
+  const int o0 = (jb * Ns * r + k) * L.es;
+  const int dstep = nb * L.es;
+  for (int l0 = 0; l0 < L.nl; l0 += Gt * ML) {
+    cplx<R> re[ML][MU], im[ML][MU];
+    bool lok[ML];
+#pragma unroll
+    for (int i = 0; i < ML; i++) {
+      const int l = l0 + lt + Gt * i;
+      lok[i] = live && l < L.nl;
+      const cplx<R> a0 = lok[i] ? buf[l * L.ls + j * L.es] : mk<R>(0, 0);
+#pragma unroll
+      for (int m = 0; m < MU; m++) {
+        re[i][m] = a0;
+        im[i][m] = mk<R>(0, 0);
+      }
+    }
+    if (live) {
+      int idx[MU];
+#pragma unroll
+      for (int m = 0; m < MU; m++) idx[m] = 0;
+      const cplx<R>* pp = buf + (l0 + lt) * L.ls + j * L.es;
+      const cplx<R>* pq = pp + r * dstep;
+      for (int s = 1; s <= H; s++) {
+        pp += dstep;
+        pq -= dstep;
+        cplx<R> P[ML], Q[ML];
+#pragma unroll
+        for (int i = 0; i < ML; i++) {
+          if (lok[i]) {
+            P[i] = pp[Gt * i * L.ls];
+            Q[i] = pq[Gt * i * L.ls];
+          } else {
+            P[i] = Q[i] = mk<R>(0, 0);
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < MU; m++) {
+          idx[m] += (u0 + m) * nb;
+          if (idx[m] >= n) idx[m] -= n;
+          const cplx<R> w = tw[idx[m]];  // (cos, -sin)(2 pi us / r)
+#pragma unroll
+          for (int i = 0; i < ML; i++) {
+            re[i][m].x += w.x * P[i].x;
+            re[i][m].y += w.x * P[i].y;
+            im[i][m].x -= w.y * Q[i].x;
+            im[i][m].y -= w.y * Q[i].y;
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < ML; i++) {
+      if (!lok[i]) continue;
+      cplx<R>* base = buf + (l0 + lt + Gt * i) * L.ls + o0;
+#pragma unroll
+      for (int m = 0; m < MU; m++) {
+        const int u = u0 + m;
+        if (u > H) break;
+        const cplx<R> rr = rot_mi(im[i][m], inv);
+        base[u * ostep] = cadd(re[i][m], rr);
+        if (u > 0) base[(r - u) * ostep] = csub(re[i][m], rr);
+      }
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+template <typename R> struct PrimeBlock;
+template <> struct PrimeBlock<float> { static constexpr int mu = 4, ml = 4; };
+template <> struct PrimeBlock<double> { static constexpr int mu = 2, ml = 4; };
+
+// Passes for radix 7, 11, 13 and primes >= 17.
+template <typename R, int EMAX>
+__device__ __forceinline__ void rare_pass(cplx<R>* buf, int n, int r, int Ns, LineSet L, const cplx<R>* tw,
+                                       bool inv) {
+  switch (r) {
+    case 7: stockham_pass<R, 7, (EMAX / 7 > 0 ? EMAX / 7 : 1)>(buf, n, Ns, L, tw, inv); break;
+    case 11: stockham_pass<R, 11, 1>(buf, n, Ns, L, tw, inv); break;
+    case 13: stockham_pass<R, 13, 1>(buf, n, Ns, L, tw, inv); break;
+    default:
+      if (!prime_pass<R, PrimeBlock<R>::mu, PrimeBlock<R>::ml>(buf, n, r, Ns, L, tw, inv))
+        generic_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv);
+      break;
+  }
+}
+
 // Full transform of all lines along one axis.  RARE selects whether the passes
 // for radix 7, 11, 13 and large primes are compiled in: they are register hungry,
 // so kernels for grids whose lengths factor into 2, 3, 4, 5, 8 leave them out
@@ -349,14 +502,7 @@ __device__ __forceinline__ void fft_lines(cplx<R>* buf, const AxisPlan P, LineSe
       case 5: stockham_pass<R, 5, MB5>(buf, n, Ns, L, tw, inv); break;
       case 8: stockham_pass<R, 8, EMAX / 8>(buf, n, Ns, L, tw, inv); break;
       default:
-        if constexpr (RARE) {
-          switch (r) {
-            case 7: stockham_pass<R, 7, (EMAX / 7 > 0 ? EMAX / 7 : 1)>(buf, n, Ns, L, tw, inv); break;
-            case 11: stockham_pass<R, 11, 1>(buf, n, Ns, L, tw, inv); break;
-            case 13: stockham_pass<R, 13, 1>(buf, n, Ns, L, tw, inv); break;
-            default: generic_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv); break;
-          }
-        }
+        if constexpr (RARE) rare_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv);
         break;
     }
     Ns *= r;

@@ -111,3 +111,30 @@ def test_metric_grid_qbq_properties():
     assert rel(q, x / eps) < 1e-12
     q32, _ = _run(ctx, fb.OP_QBQ, k, x, 2 * N, fb.MIXED)
     assert rel(q32, x / eps) < 1e-5
+
+
+@pytest.mark.parametrize("grid", [(23, 19, 34), (34, 23, 19), (17, 38, 21)])
+def test_prime_axis_lengths_match_oracle(grid):
+    """Axis lengths with prime factors >= 17 (alone, and after a radix-2 or radix-3
+    pass, so the prime pass runs with and without Stockham twiddles) in the plane
+    and the pencil stages: a simple-cubic lattice with a random B, FP64 within 1e-12
+    and FP32 within 1e-5 of the oracle."""
+    N = int(np.prod(grid))
+    par = dict(grid=grid, mesh_len=np.array([1.0 / g for g in grid]),
+               lattice_vec_a=np.array([1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0]), simple=True,
+               m=(0, 0, 0, 0), t1=np.zeros(3))
+    ctx = fb.Context.from_par(par)
+    rng = np.random.default_rng(13)
+    B = rng.uniform(1.0, 13.0, 3 * N)
+    ctx.set_eps(B)
+    k = np.array([0.3, -0.2, 0.45]) * 2 * np.pi
+    L = fo.lambdas(k, par)
+    x = rng.standard_normal(2 * L.Nd) + 1j * rng.standard_normal(2 * L.Nd)
+    v = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
+    for prec, tol in ((fb.FP64, 1e-12), (fb.MIXED, 1e-5)):
+        y, _ = _run(ctx, fb.OP_QR, k, x, 3 * N, prec)
+        assert rel(y, fo.Qr(x, L)) < tol
+        y, _ = _run(ctx, fb.OP_QRS, k, v, 2 * L.Nd, prec)
+        assert rel(y, fo.Qrs(v, L)) < tol
+        y, _ = _run(ctx, fb.OP_QBQ, k, x, 2 * L.Nd, prec)
+        assert rel(y, fo.QBQ(x, L, 1.0 / B)) < tol
