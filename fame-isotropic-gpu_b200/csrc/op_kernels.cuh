@@ -184,12 +184,13 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
   for (int i = threadIdx.x; i < Ls; i += kPencilThreads) tws[i] = a.tw[g.tws + i];
   const long fb = (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N;
-  // ---- load.  Full tiles of the Simple-lattice QBQ stream the field rows (TW
-  // contiguous elements at stride P) and the 1/eps rows straight into shared
-  // memory with 16-byte cp.async copies.
+  // ---- load.  Full tiles of the QBQ stream the field rows (TW contiguous
+  // elements at stride P) and the 1/eps rows (1/eps in the field layout) straight
+  // into shared memory with 16-byte cp.async copies.
   constexpr int CH = 16 / sizeof(cplx<R>);    // elements per 16-byte copy
   constexpr int CHB = 16 / sizeof(R);         // 1/eps values per 16-byte copy
-  const bool async_tile = MODE == PEN_QBQ && !GEN && tw_n == TW && Lf % CHB == 0;
+  const bool ib_field = !GEN || a.ib_field;  // 1/eps rows contiguous along the tile's fast positions
+  const bool async_tile = MODE == PEN_QBQ && ib_field && tw_n == TW && Lf % CHB == 0;
   if (async_tile) {
     for (int q = threadIdx.x; q < Ls * (TW / CH); q += kPencilThreads) {
       const int s = q / (TW / CH), c = q - s * (TW / CH);
@@ -243,7 +244,8 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
           else
             sp = ((long)(f0 + f) * g.Ny + m) * g.Nx + s;
           if constexpr (MODE == PEN_QBQ) {
-            const R ib = async_tile ? ibt[q] : a.invB[(long)comp * g.N + sp];
+            const long ii = ib_field ? (long)s * P + m * Lf + f0 + f : sp;
+            const R ib = async_tile ? ibt[q] : a.invB[(long)comp * g.N + ii];
             tile[q] = cscale(tile[q], ib * invN);
           } else {
             cplx<R> d;

@@ -108,6 +108,12 @@ struct fame_ctx {
   DBuf<float2> tw32;
   DBuf<double> invB64, B64;
   DBuf<float> invB32;
+  // General lattices: 1/eps also in the field layout (x, y, z; z fastest) that the
+  // pencil stage of Q_r^* B^-1 Q_r walks, so its loads are contiguous rows
+  DBuf<double> invB64q;
+  DBuf<float> invB32q;
+  const double* ibq64() const { return g.general ? invB64q.p : invB64.p; }
+  const float* ibq32() const { return g.general ? invB32q.p : invB32.p; }
   // per-batch workspace
   int cap_slots = 0, cap_nstep = 0, cap_nwant = 0;
   bool cap_mixed = false, cap_vec = false;
@@ -218,6 +224,7 @@ struct Ops {
     a.vec_per_slot = nvec;
     a.T = T;
     a.invB = invB;
+    a.ib_field = MODE == PEN_QBQ ? 1 : 0;
     a.out = out;
     a.in = in;
     a.cg = c->cg.p;
@@ -576,7 +583,7 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
              (double2*)nullptr, tol2, s.ls_maxit);
     P.while_loop(cc, [&] {
       o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr, cc);
-      o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 1);
+      o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 1);
       o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
       P.launch(k_cg_update<double>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
                (const double2*)c->p64.p, (const double2*)c->Ap64.p);
@@ -594,14 +601,14 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
       P.while_loop(inner, [&] {
         o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr,
                                          inner);
-        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 1);
+        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->ibq32(), 1);
         o.plane_fwd<float, EPI_CG, false>(c->T32.p, c->Ap32.p, 1, M, F, c->p32.p);
         P.launch(k_cg_update<float>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), c->x32.p, c->r32.p,
                  (const float2*)c->p32.p, (const float2*)c->Ap32.p);
       });
       o.plane_inv<double, IN_REFINE, false>(nullptr, c->T64.p, 1, M, F, 0, nullptr, nullptr, c->x64.p,
                                             c->x32.p);
-      o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 2);
+      o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 2);
       o.plane_fwd<double, EPI_RESID, false>(c->T64.p, c->r64.p, 1, M, F, nullptr, c->b64.p, outer, tol2);
     });
     P.launch(k_invar_epi<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j,
@@ -669,7 +676,7 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
              s.nstep, s.nstep, s.nwant, 1, c->EV.p, c0);
   // FP64 residual and Rayleigh quotient per band: v = QBQ(Sigma y)
   o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
-  o.pencil<double, PEN_QBQ>(c->Tb.p, s.nwant, F, c->invB64.p, 0);
+  o.pencil<double, PEN_QBQ>(c->Tb.p, s.nwant, F, c->ibq64(), 0);
   o.plane_fwd<double, EPI_OUT, false>(c->Tb.p, c->AV.p, s.nwant, M, F);
   P.launch(k_band_stats, dim3(1, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{}),
            (const double2*)c->EV.p, (const double2*)c->AV.p, M, s.nwant, (const double*)c->theta.p, s.nstep,
@@ -748,6 +755,10 @@ int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out) {
     c->invB64.ensure(3L * c->g.N);
     c->B64.ensure(3L * c->g.N);
     c->invB32.ensure(3L * c->g.N);
+    if (c->g.general) {
+      c->invB64q.ensure(3L * c->g.N);
+      c->invB32q.ensure(3L * c->g.N);
+    }
   } catch (const CudaError& e) {
     set_err(e.what());
     delete c;
@@ -766,10 +777,11 @@ void fame_ctx_destroy(fame_ctx* c) {
                   &c->AV, &c->Tb, &c->E})
     b->release();
   for (auto* b : {&c->r32, &c->x32, &c->p32, &c->Ap32, &c->T32, &c->tw32}) b->release();
-  for (auto* b : {&c->invB64, &c->B64, &c->partials, &c->T0, &c->T1, &c->hcoef, &c->theta, &c->Z, &c->G,
+  for (auto* b : {&c->invB64, &c->invB64q, &c->B64, &c->partials, &c->T0, &c->T1, &c->hcoef, &c->theta, &c->Z, &c->G,
                   &c->stats})
     b->release();
   c->invB32.release();
+  c->invB32q.release();
   c->slots.release();
   c->cg.release();
   c->lz.release();
@@ -811,6 +823,25 @@ int fame_set_eps(fame_ctx* c, const double* B) {
     FAME_CK(cudaMemcpy(c->B64.p, B, n3 * sizeof(double), cudaMemcpyHostToDevice));
     FAME_CK(cudaMemcpy(c->invB64.p, ib.data(), n3 * sizeof(double), cudaMemcpyHostToDevice));
     FAME_CK(cudaMemcpy(c->invB32.p, ib32.data(), n3 * sizeof(float), cudaMemcpyHostToDevice));
+    if (c->g.general) {
+      // spatial edge index (z*Ny + y)*Nx + x  ->  field index (x*Ny + y)*Nz + z
+      const Geom& g = c->g;
+      std::vector<double> q(n3);
+      std::vector<float> q32(n3);
+      for (int comp = 0; comp < 3; comp++) {
+        const long cb = (long)comp * g.N;
+        for (int z = 0; z < g.Nz; z++)
+          for (int y = 0; y < g.Ny; y++)
+            for (int x = 0; x < g.Nx; x++) {
+              const long src = cb + ((long)z * g.Ny + y) * g.Nx + x;
+              const long dst = cb + ((long)x * g.Ny + y) * g.Nz + z;
+              q[dst] = ib[src];
+              q32[dst] = ib32[src];
+            }
+      }
+      FAME_CK(cudaMemcpy(c->invB64q.p, q.data(), n3 * sizeof(double), cudaMemcpyHostToDevice));
+      FAME_CK(cudaMemcpy(c->invB32q.p, q32.data(), n3 * sizeof(float), cudaMemcpyHostToDevice));
+    }
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;
@@ -1061,7 +1092,7 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
           break;
         case FAME_OP_QBQ:
           o.plane_inv<double, IN_VEC, false>(x, c->T64.p, 1, M, F, 0);
-          o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 0);
+          o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 0);
           o.plane_fwd<double, EPI_OUT, false>(c->T64.p, y, 1, M, F);
           break;
         case FAME_OP_INVAR: {
@@ -1095,7 +1126,7 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
           P.while_loop(cc, [&] {
             o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr,
                                               cc);
-            o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 1);
+            o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 1);
             o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
             P.launch(k_cg_update<double>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
                      (const double2*)c->p64.p, (const double2*)c->Ap64.p);
@@ -1128,7 +1159,7 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
           break;
         case FAME_OP_QBQ:
           o.plane_inv<float, IN_VEC, false>(x, c->T32.p, 1, M, F, 0);
-          o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 0);
+          o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->ibq32(), 0);
           o.plane_fwd<float, EPI_OUT, false>(c->T32.p, y, 1, M, F);
           break;
       }
@@ -1212,13 +1243,13 @@ int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, int nb
       if (precision == FAME_FP64) {
         o.plane_inv<double, IN_VEC, false>(c->r64.p, c->T64.p, 1, M, F, 0);
         FAME_CK(cudaEventRecord(ev[1], c->stream));
-        o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->invB64.p, 0);
+        o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 0);
         FAME_CK(cudaEventRecord(ev[2], c->stream));
         o.plane_fwd<double, EPI_OUT, false>(c->T64.p, c->x64.p, 1, M, F);
       } else {
         o.plane_inv<float, IN_VEC, false>(c->r32.p, c->T32.p, 1, M, F, 0);
         FAME_CK(cudaEventRecord(ev[1], c->stream));
-        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->invB32.p, 0);
+        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->ibq32(), 0);
         FAME_CK(cudaEventRecord(ev[2], c->stream));
         o.plane_fwd<float, EPI_OUT, false>(c->T32.p, c->x32.p, 1, M, F);
       }

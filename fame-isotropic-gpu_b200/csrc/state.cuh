@@ -131,7 +131,8 @@ struct PencilArgs {
   long fstride;
   int vec_per_slot;
   cplx<R>* T;              // field in frequency-plane layout (in/out)
-  const R* invB;           // PEN_QBQ: 1/eps per edge (3N, spatial layout); PEN_QR_OUT: optional
+  const R* invB;           // PEN_QBQ and PEN_QR_OUT (optional): 1/eps per edge, 3N
+  int ib_field;            // invB in the field layout (else the spatial layout; same for Simple lattices)
   cplx<R>* out;            // PEN_QR_OUT: spatial field out (3N per vector)
   const cplx<R>* in;       // PEN_QRS_IN: spatial field in
   const CgState* cg;       // optional activity gate
