@@ -467,8 +467,8 @@ template <typename R> struct PrimeBlock;
 template <> struct PrimeBlock<float> { static constexpr int mu = 4, ml = 4; };
 template <> struct PrimeBlock<double> { static constexpr int mu = 2, ml = 2; };
 
-// Passes for radix 7, 11, 13 and primes >= 17.
-template <typename R, int EMAX>
+// Passes for radix 7, 11, 13 (LEVEL >= 1) and primes >= 17 (LEVEL 2).
+template <typename R, int EMAX, int LEVEL>
 __device__ __forceinline__ void rare_pass(cplx<R>* buf, int n, int r, int Ns, LineSet L, const cplx<R>* tw,
                                        bool inv) {
   switch (r) {
@@ -476,18 +476,20 @@ __device__ __forceinline__ void rare_pass(cplx<R>* buf, int n, int r, int Ns, Li
     case 11: stockham_pass<R, 11, 1>(buf, n, Ns, L, tw, inv); break;
     case 13: stockham_pass<R, 13, 1>(buf, n, Ns, L, tw, inv); break;
     default:
-      if (!prime_pass<R, PrimeBlock<R>::mu, PrimeBlock<R>::ml>(buf, n, r, Ns, L, tw, inv))
-        generic_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv);
+      if constexpr (LEVEL >= 2) {
+        if (!prime_pass<R, PrimeBlock<R>::mu, PrimeBlock<R>::ml>(buf, n, r, Ns, L, tw, inv))
+          generic_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv);
+      }
       break;
   }
 }
 
-// Full transform of all lines along one axis.  RARE selects whether the passes
-// for radix 7, 11, 13 and large primes are compiled in: they are register hungry,
-// so kernels for grids whose lengths factor into 2, 3, 4, 5, 8 leave them out
-// (the host picks the instantiation from the axis plans).  EMAX bounds the
-// elements a thread stages in registers per round.
-template <typename R, int EMAX, bool RARE>
+// Full transform of all lines along one axis.  RARE selects the passes compiled
+// in beyond radix 2, 3, 4, 5, 8: none (0), radix 7, 11, 13 (1), and also primes
+// >= 17 (2).  They are register hungry, so each grid runs the lowest level its
+// axis plans need (plan_level; the host picks the instantiation).  EMAX bounds
+// the elements a thread stages in registers per round.
+template <typename R, int EMAX, int RARE>
 __device__ __forceinline__ void fft_lines(cplx<R>* buf, const AxisPlan P, LineSet L, const cplx<R>* tw,
                                           bool inv) {
   const int n = P.n;
@@ -502,7 +504,7 @@ __device__ __forceinline__ void fft_lines(cplx<R>* buf, const AxisPlan P, LineSe
       case 5: stockham_pass<R, 5, MB5>(buf, n, Ns, L, tw, inv); break;
       case 8: stockham_pass<R, 8, EMAX / 8>(buf, n, Ns, L, tw, inv); break;
       default:
-        if constexpr (RARE) rare_pass<R, EMAX>(buf, n, r, Ns, L, tw, inv);
+        if constexpr (RARE >= 1) rare_pass<R, EMAX, RARE>(buf, n, r, Ns, L, tw, inv);
         break;
     }
     Ns *= r;
@@ -621,13 +623,15 @@ __device__ __forceinline__ void sfft(cplx<R>* buf, int ls, int es, const cplx<R>
   }
 }
 
-// true when every radix of the plan has an inlined pass in fft_lines<.., false>
-inline bool plan_is_common(const AxisPlan& P) {
+// The lowest fft_lines level (RARE) that has a pass for every radix of the plan.
+inline int plan_level(const AxisPlan& P) {
+  int lv = 0;
   for (int p = 0; p < P.npass; p++) {
     const int r = P.radix[p];
-    if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) return false;
+    if (r == 2 || r == 3 || r == 4 || r == 5 || r == 8) continue;
+    lv = (r == 7 || r == 11 || r == 13) ? (lv > 1 ? lv : 1) : 2;
   }
-  return true;
+  return lv;
 }
 
 }  // namespace fame

@@ -17,7 +17,10 @@ constexpr int kPencilThreads = 256;     // threads of a pencil CTA
 struct DynGeom {
   static constexpr bool kStatic = false;
   static constexpr int kMaxPlaneThreads = kPlaneThreads;
-  static constexpr int kMinPlaneBlocks = 1;
+  // The stage kernels' register budgets (launch bounds in op_kernels.cuh) are
+  // sized for two resident plane CTAs per SM (64 registers at 512 threads) and
+  // three pencil CTAs (85 registers), except that plane kernels with the prime
+  // pass (RARE 2), whose MU x ML accumulator block needs more, take one.
   __device__ __forceinline__ static int plane_threads() { return blockDim.x; }
   __device__ __forceinline__ static int Lf(const Geom& g) { return g.Lf; }
   __device__ __forceinline__ static int Lm(const Geom& g) { return g.Lm; }
@@ -27,13 +30,13 @@ struct DynGeom {
   // lines of a plane (pitch S) along its fast axis (fast = true) or mid axis, and
   // the TW lines of a pencil tile.  One FFT call site per kernel keeps the kernel
   // within its register budget, so the plane axis is a runtime argument.
-  template <typename R, bool RARE>
+  template <typename R, int RARE>
   __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom& g, bool fast, const cplx<R>* tw,
                                                    bool inv) {
     fft_lines<R, Emax<R>::v, RARE>(b, fast ? g.pf : g.pm, fast ? LineSet{g.Lm, g.S, 1} : LineSet{g.Lf, 1, g.S},
                                    tw, inv);
   }
-  template <typename R, bool RARE>
+  template <typename R, int RARE>
   __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom& g, const cplx<R>* tw, bool inv) {
     constexpr int TW = PencilTW<R>::v;
     fft_lines<R, Emax<R>::v, RARE>(b, g.ps, LineSet{TW, 1, TW}, tw, inv);
@@ -56,7 +59,8 @@ struct StatGeom {
   // 384 = 4 threads per line of a 96 x 96 plane: every pass of the 8 x 12 plan
   // is one round with all threads busy
   static constexpr int kMaxPlaneThreads = kStatPlaneThreads;
-  static constexpr int kMinPlaneBlocks = 2;  // two FP32 plane CTAs per SM
+  // two FP32 plane CTAs per SM (80 registers), one FP64 plane CTA; three FP32 and
+  // two FP64 pencil CTAs
   __device__ __forceinline__ static constexpr int plane_threads() { return kStatPlaneThreads; }
   __device__ __forceinline__ static constexpr int Lf(const Geom&) { return LF; }
   __device__ __forceinline__ static constexpr int Lm(const Geom&) { return LM; }
@@ -64,12 +68,12 @@ struct StatGeom {
   __device__ __forceinline__ static constexpr int S(const Geom&) { return kS; }
   __device__ __forceinline__ static constexpr int P(const Geom&) { return LF * LM; }
   static_assert(LF == LM, "a static plane geometry has equal fast and mid lengths");
-  template <typename R, bool RARE>
+  template <typename R, int RARE>
   __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom&, bool fast, const cplx<R>* tw,
                                                    bool inv) {
     sfft<R, LF, LM, kStatPlaneThreads, SEmax<R>::v>(b, fast ? kS : 1, fast ? 1 : kS, tw, inv);
   }
-  template <typename R, bool RARE>
+  template <typename R, int RARE>
   __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom&, const cplx<R>* tw, bool inv) {
     constexpr int TW = PencilTW<R>::v;
     sfft<R, LSL, TW, kPencilThreads, SPenEmax<R>::v>(b, 1, TW, tw, inv);

@@ -28,8 +28,8 @@ __device__ __forceinline__ void lam_elem(const Geom& g, const double2* tab, cons
 }
 
 // One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
-template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, sizeof(R) == 4 ? GP::kMinPlaneBlocks : 1)
+template <typename R, bool GEN, int IN, bool PR, int RARE, class GP>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::kStatic ? (sizeof(R) == 4 ? 2 : 1) : (RARE >= 2 ? 1 : 2))
     k_plane_inv(PlaneInArgs<R> a) {
   FAME_COUNT_LAUNCH();
   if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(a.reset, 0);
@@ -160,8 +160,9 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
 // ------------------------------------------------------------------ pencil stage
 
 // grid = (Lm * ceil(Lf/TW), 3 * vec_per_slot, nslots), kPencilThreads threads
-template <typename R, bool GEN, int MODE, bool RARE, class GP>
-__global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
+template <typename R, bool GEN, int MODE, int RARE, class GP>
+__global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 ? 3 : 2) : 3)
+    k_pencil(PencilArgs<R> a) {
   FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geom& g = a.g;
@@ -272,8 +273,8 @@ __global__ void __launch_bounds__(256) k_pencil(PencilArgs<R> a) {
 
 // ------------------------------------------------------------------ plane stage (forward)
 
-template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, sizeof(R) == 4 ? GP::kMinPlaneBlocks : 1)
+template <typename R, bool GEN, int EPI, bool PR, int RARE, class GP>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::kStatic ? (sizeof(R) == 4 ? 2 : 1) : (RARE >= 2 ? 1 : 2))
     k_plane_fwd(PlaneOutArgs<R> a) {
   FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];

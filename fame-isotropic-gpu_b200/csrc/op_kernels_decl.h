@@ -16,9 +16,9 @@ __host__ __device__ inline size_t pencil_smem_bytes(int Ls) {
   return (sizeof(cplx<R>) + sizeof(R)) * (size_t)Ls * PencilTW<R>::v + sizeof(cplx<R>) * (size_t)Ls;
 }
 
-template <typename R, bool GEN, int IN, bool PR, bool RARE, class GP> __global__ void k_plane_inv(PlaneInArgs<R> a);
-template <typename R, bool GEN, int MODE, bool RARE, class GP> __global__ void k_pencil(PencilArgs<R> a);
-template <typename R, bool GEN, int EPI, bool PR, bool RARE, class GP> __global__ void k_plane_fwd(PlaneOutArgs<R> a);
+template <typename R, bool GEN, int IN, bool PR, int RARE, class GP> __global__ void k_plane_inv(PlaneInArgs<R> a);
+template <typename R, bool GEN, int MODE, int RARE, class GP> __global__ void k_pencil(PencilArgs<R> a);
+template <typename R, bool GEN, int EPI, bool PR, int RARE, class GP> __global__ void k_plane_fwd(PlaneOutArgs<R> a);
 
 // combinations instantiated with a static geometry (the CG / refinement hot path
 // and the operator benchmark)

@@ -2,14 +2,14 @@
 #include "op_kernels.cuh"
 
 namespace fame {
-template __global__ void k_plane_inv<float, true, IN_CG, false, false, DynGeom>(PlaneInArgs<float>);
-template __global__ void k_plane_inv<float, true, IN_VEC, false, false, DynGeom>(PlaneInArgs<float>);
-template __global__ void k_plane_inv<float, true, IN_VEC, true, false, DynGeom>(PlaneInArgs<float>);
-template __global__ void k_pencil<float, true, PEN_QBQ, false, DynGeom>(PencilArgs<float>);
-template __global__ void k_pencil<float, true, PEN_QR_OUT, false, DynGeom>(PencilArgs<float>);
-template __global__ void k_pencil<float, true, PEN_QRS_IN, false, DynGeom>(PencilArgs<float>);
-template __global__ void k_plane_fwd<float, true, EPI_CG, false, false, DynGeom>(PlaneOutArgs<float>);
-template __global__ void k_plane_fwd<float, true, EPI_OUT, false, false, DynGeom>(PlaneOutArgs<float>);
-template __global__ void k_plane_fwd<float, true, EPI_OUT, true, false, DynGeom>(PlaneOutArgs<float>);
+template __global__ void k_plane_inv<float, true, IN_CG, false, 0, DynGeom>(PlaneInArgs<float>);
+template __global__ void k_plane_inv<float, true, IN_VEC, false, 0, DynGeom>(PlaneInArgs<float>);
+template __global__ void k_plane_inv<float, true, IN_VEC, true, 0, DynGeom>(PlaneInArgs<float>);
+template __global__ void k_pencil<float, true, PEN_QBQ, 0, DynGeom>(PencilArgs<float>);
+template __global__ void k_pencil<float, true, PEN_QR_OUT, 0, DynGeom>(PencilArgs<float>);
+template __global__ void k_pencil<float, true, PEN_QRS_IN, 0, DynGeom>(PencilArgs<float>);
+template __global__ void k_plane_fwd<float, true, EPI_CG, false, 0, DynGeom>(PlaneOutArgs<float>);
+template __global__ void k_plane_fwd<float, true, EPI_OUT, false, 0, DynGeom>(PlaneOutArgs<float>);
+template __global__ void k_plane_fwd<float, true, EPI_OUT, true, 0, DynGeom>(PlaneOutArgs<float>);
 FAME_DEFINE_LAUNCH_GETTER(launches_ops_f32_general)
 }  // namespace fame

@@ -3,10 +3,10 @@
 #include "op_kernels.cuh"
 
 namespace fame {
-template __global__ void k_plane_inv<float, false, IN_CG, false, false, Stat96>(PlaneInArgs<float>);
-template __global__ void k_plane_inv<float, false, IN_VEC, false, false, Stat96>(PlaneInArgs<float>);
-template __global__ void k_pencil<float, false, PEN_QBQ, false, Stat96>(PencilArgs<float>);
-template __global__ void k_plane_fwd<float, false, EPI_CG, false, false, Stat96>(PlaneOutArgs<float>);
-template __global__ void k_plane_fwd<float, false, EPI_OUT, false, false, Stat96>(PlaneOutArgs<float>);
+template __global__ void k_plane_inv<float, false, IN_CG, false, 0, Stat96>(PlaneInArgs<float>);
+template __global__ void k_plane_inv<float, false, IN_VEC, false, 0, Stat96>(PlaneInArgs<float>);
+template __global__ void k_pencil<float, false, PEN_QBQ, 0, Stat96>(PencilArgs<float>);
+template __global__ void k_plane_fwd<float, false, EPI_CG, false, 0, Stat96>(PlaneOutArgs<float>);
+template __global__ void k_plane_fwd<float, false, EPI_OUT, false, 0, Stat96>(PlaneOutArgs<float>);
 FAME_DEFINE_LAUNCH_GETTER(launches_ops_stat96_f32)
 }  // namespace fame

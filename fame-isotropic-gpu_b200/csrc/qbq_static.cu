@@ -97,7 +97,7 @@ bool factor_axis(int n, AxisPlan& p) {
 }
 
 // Geometry of the lattice (the layout the solver's context sets up).
-int make_geom(const fame_lattice& L, Geom& g, bool& rare, int& threads) {
+int make_geom(const fame_lattice& L, Geom& g, int& rare, int& threads) {
   memset(&g, 0, sizeof(g));
   g.Nx = L.grid[0];
   g.Ny = L.grid[1];
@@ -125,7 +125,7 @@ int make_geom(const fame_lattice& L, Geom& g, bool& rare, int& threads) {
     set_last_error("axis length needs more than 10 FFT passes");
     return FAME_ERR_UNSUPPORTED;
   }
-  rare = !(plan_is_common(g.pf) && plan_is_common(g.pm) && plan_is_common(g.ps));
+  rare = std::max(plan_level(g.pf), std::max(plan_level(g.pm), plan_level(g.ps)));
   threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
   if (plane_smem_bytes<double>(g.Lf, g.Lm, g.S) > 227 * 1024) {
     set_last_error("plane exceeds one CTA");
@@ -184,7 +184,7 @@ template <typename K> cudaError_t raise_smem(K* k, size_t bytes) {
   return cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <bool GEN, bool RARE>
+template <bool GEN, int RARE>
 cudaError_t launch_qbq(const Geom& g, int threads, const Slot* slot, const double2* tabs, const double2* tw,
                        const double2* x, const double* invB, double2* T, double2* y, cudaStream_t st) {
   const long M = 2L * g.N, F = 3L * g.N;
@@ -259,7 +259,7 @@ int fame_qbq_static(const fame_lattice* lat, const double* k, const double* inv_
     return FAME_ERR_BAD_INPUT;
   }
   Geom g;
-  bool rare = false;
+  int rare = 0;
   int threads = 0;
   int rc = make_geom(*lat, g, rare, threads);
   if (rc != FAME_OK) return rc;
@@ -322,11 +322,13 @@ int fame_qbq_static(const fame_lattice* lat, const double* k, const double* inv_
   const double2* xd = (const double2*)x;
   double2* yd = (double2*)y;
   if (g.general)
-    e = rare ? launch_qbq<true, true>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
-             : launch_qbq<true, false>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st);
+    e = rare == 2   ? launch_qbq<true, 2>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
+        : rare == 1 ? launch_qbq<true, 1>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
+                    : launch_qbq<true, 0>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st);
   else
-    e = rare ? launch_qbq<false, true>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
-             : launch_qbq<false, false>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st);
+    e = rare == 2   ? launch_qbq<false, 2>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
+        : rare == 1 ? launch_qbq<false, 1>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st)
+                    : launch_qbq<false, 0>(g, threads, slot, tabs, tw, xd, inv_b, T, yd, st);
   if (e != cudaSuccess) {
     set_last_error(std::string("QBQ launch: ") + cudaGetErrorString(e));
     return FAME_ERR_CUDA;

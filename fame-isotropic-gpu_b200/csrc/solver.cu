@@ -35,6 +35,10 @@ unsigned long long launches_ops_f32_simple_rare();
 unsigned long long launches_ops_f32_general_rare();
 unsigned long long launches_ops_f64_simple_rare();
 unsigned long long launches_ops_f64_general_rare();
+unsigned long long launches_ops_f32_simple_prime();
+unsigned long long launches_ops_f32_general_prime();
+unsigned long long launches_ops_f64_simple_prime();
+unsigned long long launches_ops_f64_general_prime();
 unsigned long long launches_ops_stat96_f32();
 unsigned long long launches_ops_stat96_f64();
 unsigned long long launches_material_locate();
@@ -100,7 +104,7 @@ struct fame_ctx {
   Geom g;
   cudaStream_t stream = nullptr;
   int plane_threads = 512;
-  bool rare = false;    // some axis length has a factor outside {2, 3, 4, 5, 8}
+  int rare = 0;         // fft_lines level the axis plans need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   bool have_eps = false;
   // persistent data
@@ -196,15 +200,19 @@ struct Ops {
     const size_t sm = plane_smem<R>(g());
     dim3 grid(3 * g().Ls, nvec, nslots);
     if (g().general) {
-      auto k = c->rare ? k_plane_inv<R, true, IN, PR, true, DynGeom> : k_plane_inv<R, true, IN, PR, false, DynGeom>;
+      auto k = c->rare == 2   ? k_plane_inv<R, true, IN, PR, 2, DynGeom>
+               : c->rare == 1 ? k_plane_inv<R, true, IN, PR, 1, DynGeom>
+                              : k_plane_inv<R, true, IN, PR, 0, DynGeom>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     } else {
-      auto k = c->rare ? k_plane_inv<R, false, IN, PR, true, DynGeom> : k_plane_inv<R, false, IN, PR, false, DynGeom>;
+      auto k = c->rare == 2   ? k_plane_inv<R, false, IN, PR, 2, DynGeom>
+               : c->rare == 1 ? k_plane_inv<R, false, IN, PR, 1, DynGeom>
+                              : k_plane_inv<R, false, IN, PR, 0, DynGeom>;
       int nt = c->plane_threads;
       if constexpr (kStatInv<R, IN, PR>)
         if (c->stat96) {
-          k = k_plane_inv<R, false, IN, PR, false, Stat96>;
+          k = k_plane_inv<R, false, IN, PR, 0, Stat96>;
           nt = kStatPlaneThreads;
         }
       allow_smem(k, sm);
@@ -234,13 +242,17 @@ struct Ops {
     const int nft = (g().Lf + a.TW - 1) / a.TW;
     dim3 grid(g().Lm * nft, 3 * nvec, nslots);
     if (g().general) {
-      auto k = c->rare ? k_pencil<R, true, MODE, true, DynGeom> : k_pencil<R, true, MODE, false, DynGeom>;
+      auto k = c->rare == 2   ? k_pencil<R, true, MODE, 2, DynGeom>
+               : c->rare == 1 ? k_pencil<R, true, MODE, 1, DynGeom>
+                              : k_pencil<R, true, MODE, 0, DynGeom>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
     } else {
-      auto k = c->rare ? k_pencil<R, false, MODE, true, DynGeom> : k_pencil<R, false, MODE, false, DynGeom>;
+      auto k = c->rare == 2   ? k_pencil<R, false, MODE, 2, DynGeom>
+               : c->rare == 1 ? k_pencil<R, false, MODE, 1, DynGeom>
+                              : k_pencil<R, false, MODE, 0, DynGeom>;
       if constexpr (kStatPen<R, MODE>)
-        if (c->stat96) k = k_pencil<R, false, MODE, false, Stat96>;
+        if (c->stat96) k = k_pencil<R, false, MODE, 0, Stat96>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
     }
@@ -271,15 +283,19 @@ struct Ops {
     const size_t sm = plane_smem<R>(g());
     dim3 grid(3 * g().Ls, nvec, nslots);
     if (g().general) {
-      auto k = c->rare ? k_plane_fwd<R, true, EPI, PR, true, DynGeom> : k_plane_fwd<R, true, EPI, PR, false, DynGeom>;
+      auto k = c->rare == 2   ? k_plane_fwd<R, true, EPI, PR, 2, DynGeom>
+               : c->rare == 1 ? k_plane_fwd<R, true, EPI, PR, 1, DynGeom>
+                              : k_plane_fwd<R, true, EPI, PR, 0, DynGeom>;
       allow_smem(k, sm);
       P.launch(k, grid, dim3(c->plane_threads), sm, a);
     } else {
-      auto k = c->rare ? k_plane_fwd<R, false, EPI, PR, true, DynGeom> : k_plane_fwd<R, false, EPI, PR, false, DynGeom>;
+      auto k = c->rare == 2   ? k_plane_fwd<R, false, EPI, PR, 2, DynGeom>
+               : c->rare == 1 ? k_plane_fwd<R, false, EPI, PR, 1, DynGeom>
+                              : k_plane_fwd<R, false, EPI, PR, 0, DynGeom>;
       int nt = c->plane_threads;
       if constexpr (kStatFwd<R, EPI, PR>)
         if (c->stat96) {
-          k = k_plane_fwd<R, false, EPI, PR, false, Stat96>;
+          k = k_plane_fwd<R, false, EPI, PR, 0, Stat96>;
           nt = kStatPlaneThreads;
         }
       allow_smem(k, sm);
@@ -327,7 +343,7 @@ static int setup_geom(fame_ctx* c) {
     set_err("axis length needs more than 10 FFT passes");
     return FAME_ERR_UNSUPPORTED;
   }
-  c->rare = !(plan_is_common(g.pf) && plan_is_common(g.pm) && plan_is_common(g.ps));
+  c->rare = std::max(plan_level(g.pf), std::max(plan_level(g.pm), plan_level(g.ps)));
   // the whole plane must fit one CTA's shared memory (FP64 copy)
   c->plane_threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
   c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96;
@@ -1187,7 +1203,9 @@ int fame_launch_count(fame_ctx* c, unsigned long long* out) {
     FAME_CK(cudaStreamSynchronize(c->stream));
     *out = launches_solver() + launches_ops_f32_simple() + launches_ops_f32_general() + launches_ops_f64_simple() +
            launches_ops_f64_general() + launches_ops_f32_simple_rare() + launches_ops_f32_general_rare() +
-           launches_ops_f64_simple_rare() + launches_ops_f64_general_rare() + launches_ops_stat96_f32() +
+           launches_ops_f64_simple_rare() + launches_ops_f64_general_rare() + launches_ops_f32_simple_prime() +
+           launches_ops_f32_general_prime() + launches_ops_f64_simple_prime() + launches_ops_f64_general_prime() +
+           launches_ops_stat96_f32() +
            launches_ops_stat96_f64() + launches_material_locate();
   } catch (const CudaError& e) {
     set_err(e.what());
