@@ -103,7 +103,9 @@ struct fame_ctx {
   fame_lattice lat;
   Geom g;
   cudaStream_t stream = nullptr;
-  int plane_threads = 512;
+  int plane_threads = 512;    // threads of a runtime-geometry plane CTA
+  int plane_threads32 = 512;  // the same for FP32 kernels
+  template <typename R> int plane_nt() const { return sizeof(R) == 4 ? plane_threads32 : plane_threads; }
   int rare = 0;         // fft_lines level the axis plans need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   bool have_eps = false;
@@ -204,12 +206,12 @@ struct Ops {
                : c->rare == 1 ? k_plane_inv<R, true, IN, PR, 1, DynGeom>
                               : k_plane_inv<R, true, IN, PR, 0, DynGeom>;
       allow_smem(k, sm);
-      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+      P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_inv<R, false, IN, PR, 2, DynGeom>
                : c->rare == 1 ? k_plane_inv<R, false, IN, PR, 1, DynGeom>
                               : k_plane_inv<R, false, IN, PR, 0, DynGeom>;
-      int nt = c->plane_threads;
+      int nt = c->template plane_nt<R>();
       if constexpr (kStatInv<R, IN, PR>)
         if (c->stat96) {
           k = k_plane_inv<R, false, IN, PR, 0, Stat96>;
@@ -287,12 +289,12 @@ struct Ops {
                : c->rare == 1 ? k_plane_fwd<R, true, EPI, PR, 1, DynGeom>
                               : k_plane_fwd<R, true, EPI, PR, 0, DynGeom>;
       allow_smem(k, sm);
-      P.launch(k, grid, dim3(c->plane_threads), sm, a);
+      P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_fwd<R, false, EPI, PR, 2, DynGeom>
                : c->rare == 1 ? k_plane_fwd<R, false, EPI, PR, 1, DynGeom>
                               : k_plane_fwd<R, false, EPI, PR, 0, DynGeom>;
-      int nt = c->plane_threads;
+      int nt = c->template plane_nt<R>();
       if constexpr (kStatFwd<R, EPI, PR>)
         if (c->stat96) {
           k = k_plane_fwd<R, false, EPI, PR, 0, Stat96>;
@@ -345,7 +347,14 @@ static int setup_geom(fame_ctx* c) {
   }
   c->rare = std::max(plan_level(g.pf), std::max(plan_level(g.pm), plan_level(g.ps)));
   // the whole plane must fit one CTA's shared memory (FP64 copy)
-  c->plane_threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
+  // threads of a runtime-geometry plane CTA: about 8 plane elements per thread, at
+  // most 256 when two planes fit in shared memory (more, smaller CTAs per SM hide
+  // the latency of the staged passes better), except FP64 planes with the prime
+  // pass, whose 128-register budget admits one CTA per SM
+  const int pt = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
+  const int kSmemSM = 227 * 1024;
+  c->plane_threads32 = 2 * plane_smem<float>(g) <= (size_t)kSmemSM ? std::min(pt, 256) : pt;
+  c->plane_threads = c->rare < 2 && 2 * plane_smem<double>(g) <= (size_t)kSmemSM ? std::min(pt, 256) : pt;
   c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96;
   if (plane_smem<double>(g) > 227 * 1024) {
     set_err("plane " + std::to_string(g.Lm) + "x" + std::to_string(g.Lf) + " exceeds one CTA");
