@@ -16,7 +16,7 @@ CG iterations, so L2 state between steps is irrelevant (config records "l2").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision mixed|fp64] [--batch B] [--no-fp64] [--no-cpu-baseline]
-                  [--mode solve|qbq|locate] [--nk K] [--tol T] [--no-graph]
+                  [--mode solve|qbq|locate|lattices] [--workload W] [--nk K] [--tol T] [--no-graph]
 
 --impl reference runs the reference's own FP64 CUDA build (oracle/_ref, compiled
 from the reference sources) through its own FAME_Fast_Algorithms_Driver; each
@@ -336,20 +336,72 @@ def run_ours(args):
 
 
 def run_qbq(args):
-    """Q_r^* B^-1 Q_r applies alone at 96^3 (one k off Gamma), each preceded by a
-    256 MiB L2 flush: the small case the kernel profiles in profiles/ capture."""
+    """Q_r^* B^-1 Q_r applies alone (96^3 or --workload; one k off Gamma), each
+    preceded by a 256 MiB L2 flush: the small case the kernel profiles in profiles/
+    capture."""
     import fame_b200 as fb
-    W = load_workload()
+    if args.workload == WORKLOAD:
+        W = load_workload()
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from fixtures import load_pre
+        W = load_pre(args.workload)
     ctx = fb.Context(W["grid"], W["mesh_len"], W["lattice_vec_a"], W["simple"], W["m"], W["t1"])
     ctx.set_material(W["binout"], W["material_num"], W["eps_in"], W["eps_out"])
     prec = fb.MIXED if args.precision == "mixed" else fb.FP64
     k = W["kpoints"][1]
     nb = max(1, args.batch)
     ms, st = ctx.bench_qbq(k, prec, reps=max(1, args.steps), nbatch=nb)
-    print(json.dumps({"mode": "qbq", "precision": args.precision, "grid": list(W["grid"]), "reps": args.steps,
+    print(json.dumps({"mode": "qbq", "workload": args.workload, "precision": args.precision,
+                      "grid": list(W["grid"]), "reps": args.steps,
                       "batch": nb, "ms_per_launch": round(ms, 5), "us_per_kpoint": round(ms * 1e3 / nb, 2),
                       "stage_ms": [round(x, 5) for x in st]}), flush=True)
     ctx.close()
+
+
+LATTICES = (("fcc64", 10), ("bcc48", 12), ("hex128", 16))
+
+
+def run_lattices(args):
+    """Band solves of the general-lattice workloads (FCC 64x55x52, BCC 48x45x39,
+    hexagonal 128x107x92; the reference's preprocessing outputs in tests/golden/)
+    at the tolerance of the reference's runs on the same B200 (1e-10): the non-Gamma
+    vertices of each path, mixed precision and FP64, timed with CUDA events on the
+    context's stream after one warm-up solve.  The reference's k-points/s are its own
+    measured per-k wall times from those runs (tests/golden/<name>_ref.json)."""
+    import torch
+    import fame_b200 as fb
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from fixtures import load_pre, load_ref
+    for name, nw in LATTICES:
+        par = load_pre(name)
+        ref = load_ref(name)
+        ctx = fb.Context.from_par(par)
+        ctx.set_material(par["binout"], par["material_num"], par["eps_in"], par["eps_out"])
+        k = par["kpoints"]
+        k = k[np.linalg.norm(k, axis=1) > 0]
+        line = {"mode": "lattices", "workload": name, "grid": list(par["grid"]), "nwant": nw, "nk": len(k),
+                "tol": ref["tol"],
+                "reference_kps": round(len(ref["kpoints"]) / sum(r["wall_s"] for r in ref["kpoints"]), 3)}
+        rk = {tuple(np.round(r["wave_vec"], 12)): np.array(r["freq"]) for r in ref["kpoints"]}
+        for prec, tag in ((fb.MIXED, "mixed"), (fb.FP64, "fp64")):
+            p = fb.solver_params(nwant=nw, nstep=NSTEP, es_tol=ref["tol"], ls_tol=ref["tol"], es_maxit=100,
+                                 ls_maxit=1000, precision=prec)
+            ctx.solve(k[:1], p)
+            st = torch.cuda.ExternalStream(ctx.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            o = ctx.solve(k, p)
+            e1.record(st)
+            e1.synchronize()
+            line[f"{tag}_kps"] = round(len(k) / (e0.elapsed_time(e1) / 1e3), 3)
+            errs = [np.max(np.abs(o["freq"][i] - rk[key]) / rk[key]) for i, key in
+                    enumerate(tuple(np.round(v, 12)) for v in k) if key in rk]
+            line[f"{tag}_max_rel_diff_vs_reference"] = float(max(errs)) if errs else None
+            line[f"{tag}_max_relres"] = float(np.max(o["relres"]))
+        print(json.dumps(line), flush=True)
+        ctx.close()
 
 
 def run_locate(args):
@@ -456,8 +508,11 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "qbq", "locate"],
-                    help="qbq: only time Q_r^* B^-1 Q_r applies at 96^3 (--steps applies; for kernel profiles)")
+    ap.add_argument("--mode", default="solve", choices=["solve", "qbq", "locate", "lattices"],
+                    help="qbq: only time Q_r^* B^-1 Q_r applies (--steps applies; for kernel profiles); "
+                         "lattices: band solves of the FCC, BCC and hexagonal workloads")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD] + [n for n, _ in LATTICES],
+                    help="grid of --mode qbq")
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven loops instead of the CUDA graph (launch lists under ncu)")
     ap.add_argument("--plain-nk", type=int, default=4, help="k-points of the one-at-a-time FP64 measurement")
@@ -471,6 +526,8 @@ def main():
         return run_qbq(args)
     if args.mode == "locate":
         return run_locate(args)
+    if args.mode == "lattices":
+        return run_lattices(args)
     return run_ours(args)
 
 
