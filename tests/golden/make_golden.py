@@ -6,6 +6,8 @@
     python tests/golden/make_golden.py condense OUTDIR
     python tests/golden/make_golden.py ref-big OUTDIR       # on a B200: full-size runs
     python tests/golden/make_golden.py condense-big OUTDIR
+    python tests/golden/make_golden.py ref-path OUTDIR      # on a B200: general-lattice paths
+    python tests/golden/make_golden.py condense-path OUTDIR
     python tests/golden/make_golden.py ref-adjoint OUTDIR   # on a B200: adjoint config
     python tests/golden/make_golden.py condense-adjoint OUTDIR
 
@@ -159,6 +161,44 @@ def condense_big(src, dst=GOLDEN):
             json.dump(out, f, indent=1)
 
 
+# Band paths of the general lattices at the reference's own path resolution:
+# hexagonal 128 with part_num 6 (5 k-points per segment, segment end excluded, on
+# Gamma-M, M-K, K-Gamma, Gamma-A: the path's first 20 points) and BCC 48 with
+# part_num 16 (15 per segment on Gamma-H, H-N, N-Gamma, Gamma-P: the first 60).
+# (name, fixture name, part_num, number of leading path points, tolerance)
+PATH_RUNS = [
+    ("hex128", "hex128_path", 6, 20, 1e-10),
+    ("bcc48", "bcc48_path", 16, 60, 1e-10),
+]
+
+
+def do_ref_path(outdir):
+    os.makedirs(outdir, exist_ok=True)
+    for name, fix, pn, nk, tol in PATH_RUNS:
+        with tempfile.TemporaryDirectory() as d:
+            ri.make_workdir(name, d, es_tol=tol, ls_tol=tol, part_num=pn)
+            out = os.path.join(outdir, f"{fix}_ref.jsonl")
+            cmd = [ri.REF_HARNESS, "solve", d, out, "--kidx", ",".join(str(i) for i in range(nk))]
+            with open(os.path.join(outdir, f"{fix}_ref.log"), "w") as log:
+                subprocess.run(cmd, check=True, stdout=log, stderr=subprocess.STDOUT)
+        print("done", fix, flush=True)
+
+
+def condense_path(src, dst=GOLDEN):
+    meta = open(os.path.join(src, "gpu.txt")).read().strip().splitlines()
+    for name, fix, pn, nk, tol in PATH_RUNS:
+        recs = [json.loads(l) for l in open(os.path.join(src, f"{fix}_ref.jsonl"))]
+        out = dict(workload=name, device=meta[1].split(",")[0], host_cores=int(meta[2]),
+                   note=f"reference FP64 CUDA build (oracle/_ref/fame_ref_harness solve), part_num={pn}, "
+                        f"first {nk} path points, es_tol=ls_tol={tol:g}, es_maxit=100, ls_maxit=1000",
+                   part_num=pn, tol=tol,
+                   kpoints=[dict(k=r["k"], wave_vec=r["wave_vec"], Nd=r["Nd"], freq=r["freq"],
+                                 ls_iter=r["ls_iter"], es_iter=r["es_iter"], wall_s=r["wall_s"])
+                            for r in recs])
+        with open(os.path.join(dst, f"{fix}_ref.json"), "w") as f:
+            json.dump(out, f, indent=1)
+
+
 # Adjoint check configuration: simple cubic 32^3, one permittivity per voxel drawn
 # uniform in [1, 13] from numpy.random.default_rng(0), 8 bands at k = (0.25, 0, 0)
 # (Cartesian, without 2*pi), tolerances 1e-12.
@@ -243,6 +283,10 @@ if __name__ == "__main__":
         do_ref_big(sys.argv[2])
     elif sys.argv[1] == "condense-big":
         condense_big(sys.argv[2])
+    elif sys.argv[1] == "ref-path":
+        do_ref_path(sys.argv[2])
+    elif sys.argv[1] == "condense-path":
+        condense_path(sys.argv[2])
     elif sys.argv[1] == "ref-adjoint":
         do_ref_adjoint(sys.argv[2])
     elif sys.argv[1] == "condense-adjoint":
