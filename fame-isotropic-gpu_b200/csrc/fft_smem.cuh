@@ -382,8 +382,11 @@ __device__ __forceinline__ bool prime_pass(cplx<R>* buf, int n, int r, int Ns, L
     }
   }
   __syncthreads();
-  // phase B
-  const int Gt = min(L.nl, T / cells);
+  // phase B: rounds of equal size (a thread's ML line slots beyond the last line
+  // would issue FMAs on zeros)
+  const int gmax = min(L.nl, T / cells);
+  const int rounds = (L.nl + gmax * ML - 1) / (gmax * ML);
+  const int Gt = ((L.nl + rounds - 1) / rounds + ML - 1) / ML;
   const int t = threadIdx.x;
   const int cell = t / Gt;
   const int lt = t - cell * Gt;
