@@ -62,6 +62,34 @@ def test_static_scratch_qbq_matches_context_qbq(name):
 
 
 @pytest.mark.gpu
+def test_static_scratch_qbq_prime_axis_lengths():
+    """A 23 x 19 x 34 simple-cubic grid (prime factors 23, 19, 17: the prime-pass
+    kernels) with a random 1/eps, against the context's FP64 QBQ."""
+    torch = pytest.importorskip("torch")
+    grid = (23, 19, 34)
+    N = int(np.prod(grid))
+    par = dict(grid=grid, mesh_len=[1.0 / g for g in grid], lattice_vec_a=[1, 0, 0, 0, 1, 0, 0, 0, 1],
+               simple=True, m=(0, 0, 0, 0), t1=np.zeros(3))
+    ctx = fb.Context.from_par(par)
+    rng = np.random.default_rng(17)
+    B = rng.uniform(1.0, 13.0, 3 * N)
+    ctx.set_eps(B)
+    inv_b = torch.from_numpy(1.0 / B).to("cuda", torch.float64)
+    lat = _lattice(par)
+    k = np.array([0.3, -0.2, 0.45])
+    x = rng.standard_normal(2 * N) + 1j * rng.standard_normal(2 * N)
+    xd = torch.from_numpy(x).to("cuda")
+    y_static = torch.full((2 * N,), np.nan, dtype=torch.complex128, device="cuda")
+    y_ctx = torch.zeros(2 * N, dtype=torch.complex128, device="cuda")
+    fb.qbq_static(lat, k, inv_b, xd, y_static)
+    torch.cuda.synchronize()
+    assert ctx.apply(fb.OP_QBQ, k, xd, y_ctx, fb.FP64) == N
+    a, b = y_static.cpu().numpy(), y_ctx.cpu().numpy()
+    assert np.all(np.isfinite(a))
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+
+
+@pytest.mark.gpu
 def test_static_scratch_qbq_matches_reference_fixture():
     torch = pytest.importorskip("torch")
     par = load_pre("sc16")
