@@ -106,6 +106,12 @@ template <typename T> __device__ __forceinline__ void cp_async_elem(T* smem, con
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
+// close this thread's current group of copies (possibly empty)
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's most recent groups are still in flight
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Kernels launched on the device, counted by each kernel's first thread.  Every
 // translation unit has its own counter; FAME_DEFINE_LAUNCH_GETTER exposes it.

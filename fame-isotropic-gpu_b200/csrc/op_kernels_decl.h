@@ -16,7 +16,14 @@ __host__ __device__ inline size_t pencil_smem_bytes(int Ls) {
   return (sizeof(cplx<R>) + sizeof(R)) * (size_t)Ls * PencilTW<R>::v + sizeof(cplx<R>) * (size_t)Ls;
 }
 
+// shared memory of a pipelined pencil CTA: two (tile, 1/eps tile) buffers | twiddles [Ls]
+template <typename R>
+__host__ __device__ inline size_t pencil_pipe_smem_bytes(int Ls) {
+  return 2 * (sizeof(cplx<R>) + sizeof(R)) * (size_t)Ls * PencilTW<R>::v + sizeof(cplx<R>) * (size_t)Ls;
+}
+
 template <typename R, bool GEN, int IN, bool PR, int RARE, class GP> __global__ void k_plane_inv(PlaneInArgs<R> a);
+template <typename R> __global__ void k_pencil_pipe(PencilArgs<R> a);
 template <typename R, bool GEN, int MODE, int RARE, class GP> __global__ void k_pencil(PencilArgs<R> a);
 template <typename R, bool GEN, int EPI, bool PR, int RARE, class GP> __global__ void k_plane_fwd(PlaneOutArgs<R> a);
 

@@ -6,9 +6,9 @@ namespace fame {
 template __global__ void k_plane_inv<double, false, IN_CG, false, 0, Stat96>(PlaneInArgs<double>);
 template __global__ void k_plane_inv<double, false, IN_VEC, false, 0, Stat96>(PlaneInArgs<double>);
 template __global__ void k_plane_inv<double, false, IN_REFINE, false, 0, Stat96>(PlaneInArgs<double>);
-template __global__ void k_pencil<double, false, PEN_QBQ, 0, Stat96>(PencilArgs<double>);
 template __global__ void k_plane_fwd<double, false, EPI_CG, false, 0, Stat96>(PlaneOutArgs<double>);
 template __global__ void k_plane_fwd<double, false, EPI_OUT, false, 0, Stat96>(PlaneOutArgs<double>);
 template __global__ void k_plane_fwd<double, false, EPI_RESID, false, 0, Stat96>(PlaneOutArgs<double>);
+template __global__ void k_pencil_pipe<double>(PencilArgs<double>);
 FAME_DEFINE_LAUNCH_GETTER(launches_ops_stat96_f64)
 }  // namespace fame

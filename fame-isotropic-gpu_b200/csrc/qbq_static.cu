@@ -224,6 +224,7 @@ cudaError_t launch_qbq(const Geom& g, int threads, const Slot* slot, const doubl
   ap.T = T;
   ap.invB = invB;
   ap.ib_field = 0;  // the caller's 1/eps is in the spatial layout
+  ap.nslots = 1;
   ap.TW = TW;
   const int nft = (g.Lf + TW - 1) / TW;
   kpen<<<dim3(g.Lm * nft, 3, 1), dim3(kPencilThreads), sm_pen, st>>>(ap);

@@ -106,6 +106,7 @@ struct fame_ctx {
   int plane_threads = 512;    // threads of a runtime-geometry plane CTA
   int plane_threads32 = 512;  // the same for FP32 kernels
   template <typename R> int plane_nt() const { return sizeof(R) == 4 ? plane_threads32 : plane_threads; }
+  int pipe_ctas64 = 0;  // resident k_pencil_pipe<double> CTAs on the device
   int rare = 0;         // fft_lines level the axis plans need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   bool have_eps = false;
@@ -152,6 +153,17 @@ template <typename R> static size_t pencil_smem(const Geom& g) { return pencil_s
 
 template <typename K> static void allow_smem(K* k, size_t bytes) {
   if (bytes > 48 * 1024) FAME_CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// CTAs of kernel k (kPencilThreads threads, `smem` dynamic shared bytes) resident on
+// the whole current device at once
+template <typename K> static int resident_ctas(K* k, size_t smem) {
+  allow_smem(k, smem);
+  int dev = 0, sms = 0, per = 0;
+  FAME_CK(cudaGetDevice(&dev));
+  FAME_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  FAME_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, kPencilThreads, smem));
+  return std::max(1, per) * sms;
 }
 
 struct Ops {
@@ -240,6 +252,7 @@ struct Ops {
     a.cg = c->cg.p;
     a.gate = gate;
     a.TW = pencil_tw<R>();
+    a.nslots = nslots;
     const size_t sm = pencil_smem<R>(g());
     const int nft = (g().Lf + a.TW - 1) / a.TW;
     dim3 grid(g().Lm * nft, 3 * nvec, nslots);
@@ -253,8 +266,19 @@ struct Ops {
       auto k = c->rare == 2   ? k_pencil<R, false, MODE, 2, DynGeom>
                : c->rare == 1 ? k_pencil<R, false, MODE, 1, DynGeom>
                               : k_pencil<R, false, MODE, 0, DynGeom>;
-      if constexpr (kStatPen<R, MODE>)
+      if constexpr (kStatPen<R, MODE> && sizeof(R) == 4)
         if (c->stat96) k = k_pencil<R, false, MODE, 0, Stat96>;
+      if constexpr (kStatPen<R, MODE> && sizeof(R) == 8)
+        if (c->stat96) {
+          // FP64: pipelined, as many CTAs as are resident, each walking tiles (the FP32
+          // stage measured no faster this way: 13.5 against 13.1 us per k-point)
+          auto kp = k_pencil_pipe<R>;
+          const size_t smp = pencil_pipe_smem_bytes<R>(g().Ls);
+          allow_smem(kp, smp);
+          const int total = (int)(grid.x * grid.y * grid.z);
+          P.launch(kp, dim3(std::min(total, c->pipe_ctas64)), dim3(kPencilThreads), smp, a);
+          return;
+        }
       allow_smem(k, sm);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
     }
@@ -356,6 +380,7 @@ static int setup_geom(fame_ctx* c) {
   c->plane_threads32 = 2 * plane_smem<float>(g) <= (size_t)kSmemSM ? std::min(pt, 256) : pt;
   c->plane_threads = c->rare < 2 && 2 * plane_smem<double>(g) <= (size_t)kSmemSM ? std::min(pt, 256) : pt;
   c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96;
+  if (c->stat96) c->pipe_ctas64 = resident_ctas(k_pencil_pipe<double>, pencil_pipe_smem_bytes<double>(g.Ls));
   if (plane_smem<double>(g) > 227 * 1024) {
     set_err("plane " + std::to_string(g.Lm) + "x" + std::to_string(g.Lf) + " exceeds one CTA");
     return FAME_ERR_UNSUPPORTED;

@@ -138,6 +138,7 @@ struct PencilArgs {
   const CgState* cg;       // optional activity gate
   int gate;                // 0 none, 1 CG active, 2 outer refinement active
   int TW;                  // fast positions per CTA
+  int nslots;              // k-points of the launch (k_pencil_pipe walks all their tiles)
 };
 
 template <typename R>
