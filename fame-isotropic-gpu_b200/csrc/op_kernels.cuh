@@ -78,11 +78,24 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   R beta = 0;
   bool first = false;
   R rscale = 0;
+  // CG step size a of the last update: the solution update x += a p is applied here
+  // (IN_CG: the previous iteration's, IN_REFINE: the inner solve's last) instead of
+  // in the vector update kernel, where it would cost another pass over p and x
+  R are = 0, aim = 0;
   if constexpr (IN == IN_CG) {
     first = st->iter == 1;
     beta = (R)st->beta;
+    are = (R)st->a_re;
+    aim = (R)st->a_im;
   }
-  if constexpr (IN == IN_REFINE) rscale = (R)(1.0 / st->scale);
+  float fre = 0.f, fim = 0.f;
+  bool pend = false;
+  if constexpr (IN == IN_REFINE) {
+    rscale = (R)(1.0 / st->scale);
+    pend = st->iter > 1;
+    fre = (float)st->a_re;
+    fim = (float)st->a_im;
+  }
   for (int e = e0 + threadIdx.x; e < e1; e += GP::plane_threads()) {
     const int fi = s * P + e;
     const int m = e / Lf, f = e - m * Lf;
@@ -107,13 +120,27 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
           x2 = r2;
         } else {
           const cplx<R> p1 = a.p[vb + i], p2 = a.p[vb + Nd + i];
+          cplx<R> s1 = a.x[vb + i], s2 = a.x[vb + Nd + i];
+          s1.x += are * p1.x - aim * p1.y;
+          s1.y += are * p1.y + aim * p1.x;
+          s2.x += are * p2.x - aim * p2.y;
+          s2.y += are * p2.y + aim * p2.x;
+          a.x[vb + i] = s1;
+          a.x[vb + Nd + i] = s2;
           x1 = mk<R>(r1.x + beta * p1.x, r1.y + beta * p1.y);
           x2 = mk<R>(r2.x + beta * p2.x, r2.y + beta * p2.y);
         }
         a.p[vb + i] = x1;
         a.p[vb + Nd + i] = x2;
       } else {  // IN_REFINE (R = double): y += x32 / scale, mix y
-        const float2 c1 = a.x32[vb + i], c2 = a.x32[vb + Nd + i];
+        float2 c1 = a.x32[vb + i], c2 = a.x32[vb + Nd + i];
+        if (pend) {
+          const float2 q1 = a.p32[vb + i], q2 = a.p32[vb + Nd + i];
+          c1.x += fre * q1.x - fim * q1.y;
+          c1.y += fre * q1.y + fim * q1.x;
+          c2.x += fre * q2.x - fim * q2.y;
+          c2.y += fre * q2.y + fim * q2.x;
+        }
         double2 y1 = a.y64[vb + i], y2 = a.y64[vb + Nd + i];
         y1.x += (double)c1.x * rscale;
         y1.y += (double)c1.y * rscale;

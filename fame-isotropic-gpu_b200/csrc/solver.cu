@@ -193,7 +193,8 @@ struct Ops {
   template <typename R, int IN, bool PR>
   void plane_inv(const cplx<R>* in, cplx<R>* T, int nvec, long vstride, long fstride, int sigma,
                  cplx<R>* p = nullptr, const cplx<R>* r = nullptr, double2* y64 = nullptr,
-                 const float2* x32 = nullptr, Cond reset = Cond{}) {
+                 const float2* x32 = nullptr, Cond reset = Cond{}, cplx<R>* x = nullptr,
+                 const float2* p32 = nullptr) {
     PlaneInArgs<R> a;
     a.reset = reset;
     a.g = g();
@@ -209,6 +210,8 @@ struct Ops {
     a.cg = c->cg.p;
     a.y64 = y64;
     a.x32 = x32;
+    a.x = x;
+    a.p32 = p32;
     a.sigma = sigma;
     a.T = T;
     const size_t sm = plane_smem<R>(g());
@@ -632,14 +635,15 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
     P.launch(k_invar_pro<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), L, j, c->r64.p, c->x64.p,
              (double2*)nullptr, tol2, s.ls_maxit);
     P.while_loop(cc, [&] {
-      o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr, cc);
+      o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr, cc,
+                                        c->x64.p);
       o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 1);
       o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
-      P.launch(k_cg_update<double>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
-               (const double2*)c->p64.p, (const double2*)c->Ap64.p);
+      P.launch(k_cg_update<double>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), c->r64.p,
+               (const double2*)c->Ap64.p);
     });
     P.launch(k_invar_epi<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j,
-             (const double2*)c->x64.p);
+             (const double2*)c->x64.p, (const double2*)c->p64.p);
   } else {
     Cond outer = loop_cond(P, flag_base, kLoopOuter, 42);
     Cond inner = loop_cond(P, flag_base, kLoopInner, s.inner_maxit + 2);
@@ -650,19 +654,19 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
                c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit, tol2, outer);
       P.while_loop(inner, [&] {
         o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr,
-                                         inner);
+                                         inner, c->x32.p);
         o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->ibq32(), 1);
         o.plane_fwd<float, EPI_CG, false>(c->T32.p, c->Ap32.p, 1, M, F, c->p32.p);
-        P.launch(k_cg_update<float>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), c->x32.p, c->r32.p,
-                 (const float2*)c->p32.p, (const float2*)c->Ap32.p);
+        P.launch(k_cg_update<float>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), c->r32.p,
+                 (const float2*)c->Ap32.p);
       });
       o.plane_inv<double, IN_REFINE, false>(nullptr, c->T64.p, 1, M, F, 0, nullptr, nullptr, c->x64.p,
-                                            c->x32.p);
+                                            c->x32.p, Cond{}, nullptr, c->p32.p);
       o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 2);
       o.plane_fwd<double, EPI_RESID, false>(c->T64.p, c->r64.p, 1, M, F, nullptr, c->b64.p, outer, tol2);
     });
     P.launch(k_invar_epi<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j,
-             (const double2*)c->x64.p);
+             (const double2*)c->x64.p, (const double2*)nullptr);
   }
   const int ndots = (int)((M + kLzRows - 1) / kLzRows);
   P.launch(k_lz_dots, dim3(ndots, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j);
@@ -1175,14 +1179,14 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
                    (double2*)nullptr, s.ls_tol * s.ls_tol, s.ls_maxit);
           P.while_loop(cc, [&] {
             o.plane_inv<double, IN_CG, false>(nullptr, c->T64.p, 1, M, F, 0, c->p64.p, c->r64.p, nullptr, nullptr,
-                                              cc);
+                                              cc, c->x64.p);
             o.pencil<double, PEN_QBQ>(c->T64.p, 1, F, c->ibq64(), 1);
             o.plane_fwd<double, EPI_CG, false>(c->T64.p, c->Ap64.p, 1, M, F, c->p64.p);
-            P.launch(k_cg_update<double>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), c->x64.p, c->r64.p,
-                     (const double2*)c->p64.p, (const double2*)c->Ap64.p);
+            P.launch(k_cg_update<double>, dim3(nvb, 1, 1), dim3(256), 0, o.va(cc), c->r64.p,
+                     (const double2*)c->Ap64.p);
           });
           P.launch(k_invar_epi<false>, dim3(nvb, 1, 1), dim3(256), 0, o.va(Cond{}), L, 0,
-                   (const double2*)c->x64.p);
+                   (const double2*)c->x64.p, (const double2*)c->p64.p);
           FAME_CK(cudaMemcpyAsync(y, c->U.p + M, 2L * sl.Nd * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
           break;
         }

@@ -76,8 +76,7 @@ struct VecArgs {
 // x += a p ; r -= a Ap ; r1 = <r, r>  (FAME_Main/CG.cu:330-341); then beta, the
 // iteration counter and the loop test r1 > tol^2 && k <= maxit (:302).
 template <typename R>
-__global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* x, cplx<R>* r,
-                                                   const cplx<R>* p, const cplx<R>* Ap) {
+__global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* r, const cplx<R>* Ap) {
   FAME_COUNT_LAUNCH();
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
@@ -89,13 +88,10 @@ __global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* x, cplx<
     const R are = (R)st->a_re, aim = (R)st->a_im;
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-      const cplx<R> pp = p[b + i], ap = Ap[b + i];
-      cplx<R> xx = x[b + i], rr = r[b + i];
-      xx.x += are * pp.x - aim * pp.y;
-      xx.y += are * pp.y + aim * pp.x;
+      const cplx<R> ap = Ap[b + i];
+      cplx<R> rr = r[b + i];
       rr.x -= are * ap.x - aim * ap.y;
       rr.y -= are * ap.y + aim * ap.x;
-      x[b + i] = xx;
       r[b + i] = rr;
       acc[0] += (double)cabs2(rr);
     }
@@ -267,7 +263,8 @@ __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r6
 // alpha_j = Re<w, u_j> (Lanczos_decomp_gpu.cu:307-309); profile counters
 // (…invAr.cu:41-43: ls_iter += k, es_iter++).
 template <bool MIXED>
-__global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, const double2* x64) {
+__global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, const double2* x64,
+                                                   const double2* p64) {
   FAME_COUNT_LAUNCH();
   const int slot = blockIdx.z;
   const Slot sl = va.slots[slot];
@@ -277,10 +274,21 @@ __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, 
   const double2* u = ucol(L, slot, j);
   double2* w = ucol(L, slot, j + 1);
   const int Nd = sl.Nd, n = 2 * Nd;
+  // plain FP64: the CG's last solution update x += a p (applied by the next
+  // iteration's plane stage, which this solve does not run)
+  const CgState* cs = va.cg + slot;
+  const bool pend = !MIXED && cs->iter > 1;
+  const double are = cs->a_re, aim = cs->a_im;
   double acc[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double s = lq_sqrt_at(va.g, tab, full_index(i, Nd, sl.off));
-    const double2 v = make_double2(x64[b + i].x / s, x64[b + i].y / s);
+    double2 xx = x64[b + i];
+    if (pend) {
+      const double2 pp = p64[b + i];
+      xx.x += are * pp.x - aim * pp.y;
+      xx.y += are * pp.y + aim * pp.x;
+    }
+    const double2 v = make_double2(xx.x / s, xx.y / s);
     w[i] = v;
     acc[0] += v.x * u[i].x + v.y * u[i].y;
   }

@@ -114,9 +114,11 @@ struct PlaneInArgs {
   const cplx<R>* in;      // IN_VEC: reduced input
   cplx<R>* p;             // IN_CG: search direction (updated in place)
   const cplx<R>* r;       // IN_CG: residual
+  cplx<R>* x;             // IN_CG: solution; takes the previous iteration's a * p here
   CgState* cg;            // IN_CG / IN_REFINE
   double2* y64;           // IN_REFINE: FP64 accumulated solution (updated)
   const float2* x32;      // IN_REFINE: FP32 correction
+  const float2* p32;      // IN_REFINE: the FP32 search direction of the inner solve's last update
   int sigma;              // IN_VEC: multiply the input by sqrt(Lambda_q) first (Sigma, …_Isotropic.cu:109)
   cplx<R>* T;             // output field (3 components)
   Cond reset;             // loop condition cleared by this kernel when it starts a loop body
