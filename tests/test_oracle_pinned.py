@@ -77,3 +77,25 @@ def test_solve_matches_reference_frequencies(name, kidx):
     assert np.max(np.abs(r.freq[nz] - f[nz]) / f[nz]) < 1e-9
     # same Lanczos path: identical A_r^-1 call count
     assert r.es_iter == rec["es_iter"]
+
+
+@pytest.mark.parametrize("name,fix,per_seg,nk", [("bcc48", "bcc48_path", 15, 60), ("hex128", "hex128_path", 5, 20)])
+def test_reference_band_path_fixtures(name, fix, per_seg, nk):
+    """The reference's own band-path fixtures (make_golden.py ref-path) walk the
+    workload's vertex list: per_seg points per segment, segment end excluded, the
+    segment ends at the vertices of the coarse path (tests/golden/<name>_pre.npz),
+    with evenly spaced points in between; Gamma (Nd = N - 1) is where the vertex
+    list has it."""
+    par = load_pre(name)
+    ref = load_ref(fix)
+    k = np.array([r["wave_vec"] for r in ref["kpoints"]])
+    assert k.shape == (nk, 3)
+    v = par["kpoints"]
+    for seg in range(nk // per_seg):
+        a, b = v[seg], v[seg + 1]
+        for i in range(per_seg):
+            assert np.allclose(k[seg * per_seg + i], a + (b - a) * (i / per_seg), atol=1e-12)
+    nd = np.array([r["Nd"] for r in ref["kpoints"]])
+    gamma = np.linalg.norm(k, axis=1) < 1e-3
+    assert np.all(nd[gamma] == par["N"] - 1) and np.all(nd[~gamma] == par["N"])
+    assert np.all(np.diff(np.array([r["freq"] for r in ref["kpoints"]]), axis=1) >= 0)
