@@ -22,14 +22,15 @@ import numpy as np
 _HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(_HERE, "libfame_b200.so")
 
-OK, ERR_BAD_INPUT, ERR_NO_CONVERGENCE, ERR_WATCHDOG, ERR_CUDA, ERR_NO_DEVICE, ERR_UNSUPPORTED = range(7)
+OK, ERR_BAD_INPUT, ERR_NO_CONVERGENCE, ERR_WATCHDOG, ERR_CUDA, ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_IO = range(8)
 FP64, MIXED = 0, 1
 OP_QR, OP_QRS, OP_QBQ, OP_PR, OP_PRS, OP_INVAR = range(6)
 
 # every symbol declared in include/fame_b200.h
 EXPORTS = ("fame_ctx_create", "fame_ctx_destroy", "fame_set_eps", "fame_set_material", "fame_solve_kpoints",
            "fame_apply", "fame_adjoint", "fame_ctx_sizes", "fame_last_error", "fame_version", "fame_ctx_stream",
-           "fame_launch_count", "fame_bench_qbq", "fame_qbq_static", "fame_material_locate")
+           "fame_launch_count", "fame_bench_qbq", "fame_qbq_static", "fame_material_locate",
+           "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish")
 QBQ_STATIC_SCRATCH_BYTES = 4 << 20  # FAME_QBQ_STATIC_SCRATCH_BYTES
 
 
@@ -97,11 +98,14 @@ def load():
     lib.fame_qbq_static.argtypes = [C.POINTER(Lattice), D, P, P, P, P]
     lib.fame_material_locate.argtypes = [C.c_int, C.POINTER(LocateGeometry), C.POINTER(MaterialShapes),
                                          C.POINTER(C.c_int)]
+    lib.fame_write_eigenvectors.argtypes = [C.c_char_p, D, C.c_int, C.c_longlong, C.c_int, C.c_int]
+    lib.fame_writer_start.argtypes = [C.c_char_p, D, C.c_int, C.c_longlong, C.c_int, C.c_int, C.POINTER(P)]
+    lib.fame_writer_finish.argtypes = [P]
     lib.fame_last_error.restype = C.c_char_p
     lib.fame_version.restype = C.c_char_p
     for fn in ("fame_ctx_create", "fame_set_eps", "fame_set_material", "fame_solve_kpoints", "fame_apply",
                "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq", "fame_qbq_static",
-               "fame_material_locate"):
+               "fame_material_locate", "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib
@@ -278,6 +282,18 @@ def qbq_static(lattice, k, inv_b, x, y, stream=0):
     kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
     _check(load().fame_qbq_static(C.byref(lattice), _dptr(kk), C.c_void_p(inv_b.data_ptr()),
                                   C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(stream)))
+
+
+def write_eigenvectors(evec, kidx, directory=None, nthreads=0):
+    """Data_EV_<kk>_<bb>.txt files of one wave vector in the reference's format
+    (FAME_Save_Eigenvector) through fame_write_eigenvectors: evec is (nwant, 3N)
+    complex128 on the host, kidx the 0-based wave-vector index."""
+    ev = np.ascontiguousarray(np.asarray(evec, dtype=np.complex128))
+    if ev.ndim != 2:
+        raise ValueError("evec must be (nwant, 3N)")
+    d = None if directory is None else os.fsencode(directory)
+    _check(load().fame_write_eigenvectors(d, ev.ctypes.data_as(C.POINTER(C.c_double)), ev.shape[0], ev.shape[1],
+                                          int(kidx), int(nthreads)))
 
 
 def version():

@@ -14,7 +14,9 @@
 //   * Profile->ls_iter[i] / es_iter[i] / es_time[i] per wave vector, Profile->idx
 //     left at the last wave vector, the profile table printed per wave vector;
 //   * Data_Omega_array.txt written by the reference's FAME_Create_Frequency_txt and,
-//     when Par.flag.save_eigen_vector is set, Data_EV_*.txt by FAME_Save_Eigenvector;
+//     when Par.flag.save_eigen_vector is set, Data_EV_*.txt in FAME_Save_Eigenvector's
+//     format by fame_writer_start (formatted on all host threads, written while the
+//     next wave vector is solved);
 //   * the sign convention of Check_Residual (FAME_Main_Code.cu:383-421): a frequency
 //     whose residual ||C^H C E - w^2 B E|| (E scaled as the reference restores it)
 //     exceeds 1e-10 is stored negated.  The residual comes from the solver's FP64
@@ -35,7 +37,6 @@
 
 #include "FAME_Internal_Common.h"
 #include "FAME_Create_Frequency_txt.h"
-#include "FAME_Save_Eigenvector.h"
 #include "FAME_Profile.h"
 #include "fame_b200.h"
 
@@ -115,16 +116,28 @@ int FAME_Main_Code(PAR Par, PROFILE* Profile) {
 
   std::vector<double> freq((size_t)nk * Nwant), relres((size_t)nk * Nwant), resabs((size_t)nk * Nwant);
   std::vector<fame_kcounters> cnt(nk);
-  std::vector<double> evec(save ? (size_t)Nwant * 3 * N * 2 : 0);
+  // two eigenvector buffers: the files of wave vector i are written on a background
+  // thread (fame_writer_start) while wave vector i + 1 is solved into the other
+  std::vector<double> evec[2];
+  if (save)
+    for (auto& e : evec) e.resize((size_t)Nwant * 3 * N * 2);
+  fame_writer* writer = nullptr;
+  auto finish_writer = [&]() -> int {
+    const int wrc = writer ? fame_writer_finish(writer) : FAME_OK;
+    writer = nullptr;
+    return wrc;
+  };
   int status = FAME_OK;
   for (int k0 = 0; k0 < nk; k0 += chunk) {
     const int n = nk - k0 < chunk ? nk - k0 : chunk;
+    std::vector<double>& ev = evec[(k0 / chunk) & 1];
     const double t0 = now_s();
     rc = fame_solve_kpoints(ctx, Par.recip_lattice.WaveVector + 3L * k0, n, &p, freq.data() + (size_t)k0 * Nwant,
                             relres.data() + (size_t)k0 * Nwant, nullptr, resabs.data() + (size_t)k0 * Nwant,
-                            save ? evec.data() : nullptr, cnt.data() + k0);
+                            save ? ev.data() : nullptr, cnt.data() + k0);
     const double dt = now_s() - t0;
     if (rc != FAME_OK && rc != FAME_ERR_NO_CONVERGENCE) {
+      finish_writer();
       fame_ctx_destroy(ctx);
       return fail(rc, "fame_solve_kpoints");
     }
@@ -144,9 +157,26 @@ int FAME_Main_Code(PAR Par, PROFILE* Profile) {
                relres[(size_t)i * Nwant + b]);
         if (res > 1e-10) f = -f;
       }
-      if (save) FAME_Save_Eigenvector(reinterpret_cast<cmpx*>(evec.data()), Nwant, (int)(3 * N), i);
+      if (save) {
+        // Data_EV_*.txt as FAME_Save_Eigenvector writes them (FAME_Main_Code.cu:127), byte for byte
+        const int wrc = finish_writer();
+        if (wrc != FAME_OK) {
+          fame_ctx_destroy(ctx);
+          return fail(wrc, "fame_writer_finish");
+        }
+        const int src = fame_writer_start(nullptr, ev.data(), Nwant, 3LL * N, i, 0, &writer);
+        if (src != FAME_OK) {
+          fame_ctx_destroy(ctx);
+          return fail(src, "fame_writer_start");
+        }
+      }
       FAME_Print_Profile(*Profile);
     }
+  }
+  const int wrc = finish_writer();
+  if (wrc != FAME_OK) {
+    fame_ctx_destroy(ctx);
+    return fail(wrc, "fame_writer_finish");
   }
   FAME_Create_Frequency_txt(freq.data(), Nwant, Profile->idx);
   fame_ctx_destroy(ctx);

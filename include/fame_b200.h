@@ -31,7 +31,8 @@ enum {
   FAME_ERR_WATCHDOG = 3,
   FAME_ERR_CUDA = 4,
   FAME_ERR_NO_DEVICE = 5,
-  FAME_ERR_UNSUPPORTED = 6
+  FAME_ERR_UNSUPPORTED = 6,
+  FAME_ERR_IO = 7
 };
 
 /* precision modes */
@@ -209,6 +210,25 @@ int fame_material_locate(int device, const fame_locate_geometry* geo, const fame
  * looks up the array's address; make it before any stream capture. */
 int fame_qbq_static(const fame_lattice* lat, const double* k_xyz, const double* inv_b, const void* x, void* y,
                     void* stream);
+
+/* Eigenvector text files in the reference's format: replaces FAME_Save_Eigenvector
+ * (FAME_Tools/FAME_Save_Eigenvector.cpp:7-45, called from FAME_Main/FAME_Main_Code.cu:127).
+ * For band b of wave vector kidx it writes <dir>/Data_EV_<kk>_<bb>.txt (kk = kidx + 1,
+ * bb = b + 1, at least two digits) holding the line "Ele_field_mtx{kk}(:, bb) = [",
+ * then one "(% e) + (% e * 1i)" line per entry and "];", byte for byte what the
+ * reference's writer produces.  The lines are formatted on `nthreads` host threads
+ * (0: all hardware threads) and written in order.
+ *   dir     directory (NULL or "": the working directory)
+ *   evec    host, nwant x n3 complex128 (band-major, n3 = 3N): one wave vector's
+ *           eigenvectors as fame_solve_kpoints returns them
+ * fame_writer_start does the same on a background thread and returns at once; the
+ * caller keeps `evec` unchanged until fame_writer_finish(writer) has returned, which
+ * joins the thread, frees the writer and returns the write's status. */
+typedef struct fame_writer fame_writer;
+int fame_write_eigenvectors(const char* dir, const double* evec, int nwant, long long n3, int kidx, int nthreads);
+int fame_writer_start(const char* dir, const double* evec, int nwant, long long n3, int kidx, int nthreads,
+                      fame_writer** writer_out);
+int fame_writer_finish(fame_writer* writer);
 
 const char* fame_last_error(void);
 const char* fame_version(void);

@@ -9,6 +9,8 @@
 #   oracle/_ref/fame_ref_main     the reference's own Main.cpp program
 #   oracle/_ref/fame_ref_harness  oracle/ref_harness.cu linked with every reference
 #                                 object except Main.o
+#   oracle/_ref/fame_ref_evwriter oracle/ref_evwriter.cpp with the reference's
+#                                 FAME_Save_Eigenvector
 # Only header shims are added (oracle/ref_shims/); no reference source is edited or
 # copied.  LAPACKE_zpteqr is bound to scipy's bundled OpenBLAS (LP64 LAPACKE).
 set -euo pipefail
@@ -51,4 +53,6 @@ LIBS="-L/usr/local/cuda/lib64 -lcudart -lcublas -lcufft -lpthread -ldl $OPENBLAS
 REFOBJS=$(ls "$OBJ"/*.o | grep -v -e '/Main.o$' -e '/ref_harness.o$')
 g++ -o "$OUT/fame_ref_main" "$OBJ/Main.o" $REFOBJS $LIBS
 g++ -o "$OUT/fame_ref_harness" "$OBJ/ref_harness.o" $REFOBJS $LIBS
-echo "built $OUT/fame_ref_main and $OUT/fame_ref_harness"
+# the reference's eigenvector writer alone, for the byte-for-byte writer test
+g++ -O2 -w -o "$OUT/fame_ref_evwriter" "$HERE/ref_evwriter.cpp" "$OBJ/FAME_Save_Eigenvector.o"
+echo "built $OUT/fame_ref_main, $OUT/fame_ref_harness and $OUT/fame_ref_evwriter"
