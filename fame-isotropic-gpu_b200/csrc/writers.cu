@@ -7,6 +7,7 @@
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <string>
 #include <thread>
 #include <vector>
@@ -103,7 +104,12 @@ int fame_write_eigenvectors(const char* dir, const double* evec, int nwant, long
   int rc = check(evec, nwant, n3, kidx);
   if (rc) return rc;
   std::string err;
-  rc = run_job(EvJob{dir ? dir : "", evec, nwant, n3, kidx, nthreads}, err);
+  try {
+    rc = run_job(EvJob{dir ? dir : "", evec, nwant, n3, kidx, nthreads}, err);
+  } catch (const std::exception& e) {  // thread creation or allocation
+    err = std::string("eigenvector writer: ") + e.what();
+    rc = FAME_ERR_IO;
+  }
   if (rc) fame::set_last_error(err);
   return rc;
 }
@@ -117,9 +123,23 @@ int fame_writer_start(const char* dir, const double* evec, int nwant, long long 
   *writer_out = nullptr;
   int rc = check(evec, nwant, n3, kidx);
   if (rc) return rc;
-  fame_writer* w = new fame_writer;
-  const EvJob job{dir ? dir : "", evec, nwant, n3, kidx, nthreads};
-  w->th = std::thread([w, job] { w->rc = run_job(job, w->err); });
+  fame_writer* w = nullptr;
+  try {
+    w = new fame_writer;
+    const EvJob job{dir ? dir : "", evec, nwant, n3, kidx, nthreads};
+    w->th = std::thread([w, job] {
+      try {
+        w->rc = run_job(job, w->err);
+      } catch (const std::exception& e) {
+        w->err = std::string("eigenvector writer: ") + e.what();
+        w->rc = FAME_ERR_IO;
+      }
+    });
+  } catch (const std::exception& e) {
+    delete w;
+    fame::set_last_error(std::string("eigenvector writer: ") + e.what());
+    return FAME_ERR_IO;
+  }
   *writer_out = w;
   return FAME_OK;
 }
