@@ -184,8 +184,14 @@ def cpu_baseline(W, es_mean, counters):
         finally:
             np.fft.fftn, np.fft.ifftn = saved
     per_k = t * es_mean
-    return {"value": 1.0 / per_k, "unit": "k-points/s", "cores": cores, "kind": "port",
-            "sample": f"oracle (numpy+scipy.fft FP64) A_r^-1 at 96^3 k={list(np.round(k, 4))}: "
+    cpu = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            cpu = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), "")
+    except OSError:
+        pass
+    return {"value": 1.0 / per_k, "unit": "k-points/s", "cores": cores, "kind": "port", "cpu_model": cpu,
+            "sample": f"oracle (numpy+scipy.fft FP64) A_r^-1 at 96^3 k={[float(v) for v in np.round(k, 4)]}: "
                       f"{cnt['ls_iter']} CG products in {t:.2f}s, x mean {es_mean:.1f} A_r^-1 per k "
                       f"(Lanczos reorthogonalisation not included: lower bound on CPU time)"}
 
