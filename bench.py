@@ -196,6 +196,35 @@ def cpu_baseline(W, es_mean, counters):
                       f"(Lanczos reorthogonalisation not included: lower bound on CPU time)"}
 
 
+def solve_bytes(counters, N, nwant, nstep, mixed):
+    """Algorithmic HBM bytes of a band solve, summed from its per-k counters: every
+    FP32 (mixed) or FP64 CG iteration moves B_QBQ + 7M.s (operator: x in, the field out
+    of Q_r and into Q_r^*, y out, 1/eps; CG vectors: read r, p, x, Ap, write x, r, p),
+    every FP64 refinement step B_QBQ(FP64) + 3M.16, Lanczos step j 4M.16 + 2(j+1)M.16
+    (the CGS pass reads U twice), every restart (nstep + 1 + nwant + 1)M.16 (U times the
+    rotation), and the restoration nwant(M + 6N).16, with M = 2N complex values per
+    reduced vector, s = 8 (FP32) or 16 bytes per complex value.  Lanczos step t of a k
+    has j = t for t < nstep and j = nwant + (t - nstep) mod (nstep - nwant) after a
+    restart."""
+    M = 2 * N
+
+    def qbq(s, r):
+        return (2 * M + 6 * N) * s + 3 * N * r
+
+    s, r = (8, 4) if mixed else (16, 8)
+    total = 0
+    for c in counters:
+        b = c["ls_iter"] * (qbq(s, r) + 7 * M * s)
+        if mixed:
+            b += c.get("refine", 0) * (qbq(16, 8) + 3 * M * 16)
+        js = sum(1 + (t if t < nstep else nwant + (t - nstep) % (nstep - nwant)) for t in range(c["es_iter"]))
+        b += c["es_iter"] * 4 * M * 16 + 2 * js * M * 16
+        b += c.get("restarts", 0) * (nstep + 1 + nwant + 1) * M * 16
+        b += nwant * (M + 6 * N) * 16
+        total += b
+    return total
+
+
 def run_ours(args):
     import torch
     import fame_b200 as fb
@@ -313,6 +342,17 @@ def run_ours(args):
         tpp = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist)
         fp64["one_k_at_a_time_host_loops"] = {"value": kpp.shape[0] * ws / tpp, "kpoints": int(kpp.shape[0]),
                                               "speedup_mixed_over_it": round(value / (kpp.shape[0] * ws / tpp), 3)}
+    # ---- the whole solve against HBM: algorithmic bytes from this run's counters
+    solve_roof = None
+    try:
+        sb = solve_bytes(counters, N, NWANT, NSTEP, prec == fb.MIXED)
+        t_step = dt / args.steps
+        solve_roof = {"bound": "hbm", "algorithmic_bytes_per_step": int(sb), "seconds_per_step": round(t_step, 4),
+                      "achieved": round(sb / t_step / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                      "frac": round(sb / t_step / 1e9 / hbm, 4),
+                      "counts": "CG iterations, FP64 refinements, Lanczos steps, restarts, restoration (bench.solve_bytes)"}
+    except (KeyError, TypeError, ValueError, ZeroDivisionError):
+        solve_roof = None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(W, es_mean, counters)
@@ -332,7 +372,7 @@ def run_ours(args):
             "counters": {"es_iter_mean": es_mean, "ls_iter_total": ls_sum,
                          "restarts_total": int(sum(c["restarts"] for c in counters)),
                          "fp64_refinements_total": int(sum(c["refine"] for c in counters))},
-            "roofline": roof, "plain_fp64": fp64, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roof, "solve_roofline": solve_roof, "plain_fp64": fp64, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
