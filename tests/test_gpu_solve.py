@@ -1,6 +1,6 @@
 """Full band-structure solves on the GPU against the reference's FP64 CUDA build.
 
-Bars (BASELINE: eigenvalues within relative 1e-6 at residual 1e-6):
+Bars (eigenvalues within relative 1e-6 at residual 1e-6):
   * FP64 path: frequencies within 1e-8 relative of the reference, same number of
     A_r^-1 applications (same Lanczos path);
   * mixed path (FP32 operator/CG + FP64 refinement, FP64 Lanczos): within 1e-6;
