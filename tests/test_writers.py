@@ -97,3 +97,25 @@ def test_errors_are_reported(tmp_path):
     assert lib.fame_writer_finish(w) == fb.ERR_IO
     assert "cannot open" in lib.fame_last_error().decode()
     assert lib.fame_writer_finish(None) == fb.ERR_BAD_INPUT
+
+
+def test_default_directory_is_the_working_directory(tmp_path, monkeypatch):
+    """dir = NULL writes into the working directory, as the reference's writer does;
+    two background writers run at once into different directories."""
+    monkeypatch.chdir(tmp_path)
+    v = _vectors(2, 1001, seed=5)
+    fb.write_eigenvectors(v, 4)
+    assert sorted(os.listdir(tmp_path)) == ["Data_EV_05_01.txt", "Data_EV_05_02.txt"]
+    lib = fb.load()
+    ev = np.ascontiguousarray(v)
+    ws = []
+    for d in ("a", "b"):
+        (tmp_path / d).mkdir()
+        w = C.c_void_p()
+        assert lib.fame_writer_start(os.fsencode(str(tmp_path / d)), ev.ctypes.data_as(C.POINTER(C.c_double)), 2,
+                                     1001, 4, 2, C.byref(w)) == fb.OK
+        ws.append(w)
+    for w in ws:
+        assert lib.fame_writer_finish(w) == fb.OK
+    for n in ("Data_EV_05_01.txt", "Data_EV_05_02.txt"):
+        assert _read(tmp_path / n) == _read(tmp_path / "a" / n) == _read(tmp_path / "b" / n)
