@@ -96,68 +96,102 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     fre = (float)st->a_re;
     fim = (float)st->a_im;
   }
-  for (int e = e0 + threadIdx.x; e < e1; e += GP::plane_threads()) {
-    const int fi = s * P + e;
-    const int m = e / Lf, f = e - m * Lf;
-    cplx<R> v[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
-    if (fi >= off) {
-      const long i = fi - off;
-      cplx<R> Lx, Ly, Lz;
-      lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
-      cplx<R> x1, x2;
-      if constexpr (IN == IN_VEC) {
-        x1 = a.in[vb + i];
-        x2 = a.in[vb + Nd + i];
-        if (a.sigma) {
-          const R sc = sqrt(cabs2(Lx) + cabs2(Ly) + cabs2(Lz));
-          x1 = cscale(x1, sc);
-          x2 = cscale(x2, sc);
-        }
-      } else if constexpr (IN == IN_CG) {
-        const cplx<R> r1 = a.r[vb + i], r2 = a.r[vb + Nd + i];
-        if (first) {
-          x1 = r1;
-          x2 = r2;
-        } else {
-          const cplx<R> p1 = a.p[vb + i], p2 = a.p[vb + Nd + i];
-          cplx<R> s1 = a.x[vb + i], s2 = a.x[vb + Nd + i];
-          s1.x += are * p1.x - aim * p1.y;
-          s1.y += are * p1.y + aim * p1.x;
-          s2.x += are * p2.x - aim * p2.y;
-          s2.y += are * p2.y + aim * p2.x;
-          a.x[vb + i] = s1;
-          a.x[vb + Nd + i] = s2;
-          x1 = mk<R>(r1.x + beta * p1.x, r1.y + beta * p1.y);
-          x2 = mk<R>(r2.x + beta * p2.x, r2.y + beta * p2.y);
-        }
-        a.p[vb + i] = x1;
-        a.p[vb + Nd + i] = x2;
-      } else {  // IN_REFINE (R = double): y += x32 / scale, mix y
-        float2 c1 = a.x32[vb + i], c2 = a.x32[vb + Nd + i];
-        if (pend) {
-          const float2 q1 = a.p32[vb + i], q2 = a.p32[vb + Nd + i];
-          c1.x += fre * q1.x - fim * q1.y;
-          c1.y += fre * q1.y + fim * q1.x;
-          c2.x += fre * q2.x - fim * q2.y;
-          c2.y += fre * q2.y + fim * q2.x;
-        }
-        double2 y1 = a.y64[vb + i], y2 = a.y64[vb + Nd + i];
-        y1.x += (double)c1.x * rscale;
-        y1.y += (double)c1.y * rscale;
-        y2.x += (double)c2.x * rscale;
-        y2.y += (double)c2.y * rscale;
-        a.y64[vb + i] = y1;
-        a.y64[vb + Nd + i] = y2;
-        x1 = cvt<R>(y1);
-        x2 = cvt<R>(y2);
-      }
-      cplx<R> Pc[6];
-      pi_from<R>(GEN, PR, Lx, Ly, Lz, Pc);
+  // Input stage and the 2 -> 3 mix.  IN_CG: p = r + beta p (p = r at k = 1) and the
+  // deferred x += a p (CG.cu:39-51, :65-66).  IN_REFINE: y += x32 / scale with the
+  // inner solve's last update folded in.  The operands of KB points per thread are
+  // loaded up front, so one global-load latency covers KB points.
+  // (runtime geometries run at 64 registers: two points)
+  constexpr int KB = !GP::kStatic ? 2 : IN == IN_VEC ? 8 : (sizeof(R) == 4 ? 4 : 2);
+  const int NT = GP::plane_threads();
+  for (int eb = e0 + threadIdx.x; eb < e1; eb += KB * NT) {
+    cplx<R> A1[KB], A2[KB], B1[KB], B2[KB], C1[KB], C2[KB];
+    float2 F1[KB], F2[KB], G1[KB], G2[KB];
 #pragma unroll
-      for (int c = 0; c < 3; c++) v[c] = cadd(cmul(Pc[c], x1), cmul(Pc[3 + c], x2));
+    for (int k = 0; k < KB; k++) {
+      const int e = eb + k * NT;
+      if (e < e1 && s * P + e >= off) {
+        const long i = s * P + e - off;
+        if constexpr (IN == IN_VEC) {
+          A1[k] = a.in[vb + i];
+          A2[k] = a.in[vb + Nd + i];
+        } else if constexpr (IN == IN_CG) {
+          A1[k] = a.r[vb + i];
+          A2[k] = a.r[vb + Nd + i];
+          if (!first) {
+            B1[k] = a.p[vb + i];
+            B2[k] = a.p[vb + Nd + i];
+            C1[k] = a.x[vb + i];
+            C2[k] = a.x[vb + Nd + i];
+          }
+        } else {  // IN_REFINE (R = double)
+          A1[k] = a.y64[vb + i];
+          A2[k] = a.y64[vb + Nd + i];
+          F1[k] = a.x32[vb + i];
+          F2[k] = a.x32[vb + Nd + i];
+          if (pend) {
+            G1[k] = a.p32[vb + i];
+            G2[k] = a.p32[vb + Nd + i];
+          }
+        }
+      }
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++) dst[c][m * S + f] = v[c];
+    for (int k = 0; k < KB; k++) {
+      const int e = eb + k * NT;
+      if (e >= e1) break;
+      const int fi = s * P + e;
+      const int m = e / Lf, f = e - m * Lf;
+      cplx<R> v[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
+      if (fi >= off) {
+        const long i = fi - off;
+        cplx<R> Lx, Ly, Lz;
+        lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
+        cplx<R> x1 = A1[k], x2 = A2[k];
+        if constexpr (IN == IN_VEC) {
+          if (a.sigma) {
+            const R sc = sqrt(cabs2(Lx) + cabs2(Ly) + cabs2(Lz));
+            x1 = cscale(x1, sc);
+            x2 = cscale(x2, sc);
+          }
+        } else if constexpr (IN == IN_CG) {
+          if (!first) {
+            cplx<R> s1 = C1[k], s2 = C2[k];
+            const cplx<R> p1 = B1[k], p2 = B2[k];
+            s1.x += are * p1.x - aim * p1.y;
+            s1.y += are * p1.y + aim * p1.x;
+            s2.x += are * p2.x - aim * p2.y;
+            s2.y += are * p2.y + aim * p2.x;
+            a.x[vb + i] = s1;
+            a.x[vb + Nd + i] = s2;
+            x1 = mk<R>(x1.x + beta * p1.x, x1.y + beta * p1.y);
+            x2 = mk<R>(x2.x + beta * p2.x, x2.y + beta * p2.y);
+          }
+          a.p[vb + i] = x1;
+          a.p[vb + Nd + i] = x2;
+        } else {  // IN_REFINE
+          float2 c1 = F1[k], c2 = F2[k];
+          if (pend) {
+            const float2 q1 = G1[k], q2 = G2[k];
+            c1.x += fre * q1.x - fim * q1.y;
+            c1.y += fre * q1.y + fim * q1.x;
+            c2.x += fre * q2.x - fim * q2.y;
+            c2.y += fre * q2.y + fim * q2.x;
+          }
+          x1.x += (double)c1.x * rscale;
+          x1.y += (double)c1.y * rscale;
+          x2.x += (double)c2.x * rscale;
+          x2.y += (double)c2.y * rscale;
+          a.y64[vb + i] = x1;
+          a.y64[vb + Nd + i] = x2;
+        }
+        cplx<R> Pc[6];
+        pi_from<R>(GEN, PR, Lx, Ly, Lz, Pc);
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[c] = cadd(cmul(Pc[c], x1), cmul(Pc[3 + c], x2));
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) dst[c][m * S + f] = v[c];
+    }
   }
   cl.sync();
 
@@ -167,8 +201,8 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   for (int ax = 0; ax < 2; ax++) {
     GP::template fft_plane<R, RARE>(plane, g, ax == 0, ax == 0 ? twf : twm, true);
     if constexpr (GEN) {
-      // x D_kz(x,y,z) after the z (fast) pass (FAME_FFT_CUDA.cu:278, kernel :452-487),
-      // x D_ky(x,y) after the y (mid) pass (FAME_FFT_CUDA.cu:284, kernel :367-404)
+      // x D_kz(x,y,z) after the z (fast) pass (FAME_FFT_CUDA.cu:109, kernel :283-317),
+      // x D_ky(x,y) after the y (mid) pass (FAME_FFT_CUDA.cu:115, kernel :198-234)
       for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
         const int m = e / Lf, f = e - m * Lf;
         const int q = m * S + f;
@@ -199,6 +233,7 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
   cplx<R>* tile = reinterpret_cast<cplx<R>*>(smem_raw);
   R* ibt = reinterpret_cast<R*>(tile + Ls * TW);
   cplx<R>* tws = reinterpret_cast<cplx<R>*>(ibt + Ls * TW);
+  constexpr bool QBQ = MODE == PEN_QBQ || MODE == PEN_QBQ_CG;
   const int slot = blockIdx.z;
   const Slot sl = a.slots[slot];
   if (!sl.active) return;
@@ -218,7 +253,7 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
   constexpr int CH = 16 / sizeof(cplx<R>);    // elements per 16-byte copy
   constexpr int CHB = 16 / sizeof(R);         // 1/eps values per 16-byte copy
   const bool ib_field = !GEN || a.ib_field;  // 1/eps rows contiguous along the tile's fast positions
-  const bool async_tile = MODE == PEN_QBQ && ib_field && tw_n == TW && Lf % CHB == 0;
+  const bool async_tile = QBQ && ib_field && tw_n == TW && Lf % CHB == 0;
   if (async_tile) {
     for (int q = threadIdx.x; q < Ls * (TW / CH); q += kPencilThreads) {
       const int s = q / (TW / CH), c = q - s * (TW / CH);
@@ -257,7 +292,9 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
   __syncthreads();
   // QBQ: inverse, x B^{-1}/N, forward.  QR_OUT: inverse, x D/N (and B^{-1}), store.
   // QRS_IN: forward only.  One FFT call site (dir loop) for the register budget.
-  constexpr int ndir = MODE == PEN_QBQ ? 2 : 1;
+  constexpr int ndir = QBQ ? 2 : 1;
+  // PEN_QBQ_CG: sum of |v|^2 / eps over the tile after the inverse transform
+  float dot = 0.f;
   for (int dir = 0; dir < ndir; dir++) {
     const bool inv = MODE == PEN_QRS_IN ? false : dir == 0;
     GP::template fft_slow<R, RARE>(tile, g, tws, inv);
@@ -271,9 +308,10 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
             sp = (long)s * P + m * Lf + f0 + f;
           else
             sp = ((long)(f0 + f) * g.Ny + m) * g.Nx + s;
-          if constexpr (MODE == PEN_QBQ) {
+          if constexpr (QBQ) {
             const long ii = ib_field ? (long)s * P + m * Lf + f0 + f : sp;
             const R ib = async_tile ? ibt[q] : a.invB[(long)comp * g.N + ii];
+            if constexpr (MODE == PEN_QBQ_CG) dot += (float)(ib * cabs2(tile[q]));
             tile[q] = cscale(tile[q], ib * invN);
           } else {
             cplx<R> d;
@@ -290,10 +328,31 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
       __syncthreads();
     }
   }
-  if constexpr (MODE == PEN_QBQ || MODE == PEN_QRS_IN) {
+  if constexpr (QBQ || MODE == PEN_QRS_IN) {
     for (int q = threadIdx.x; q < Ls * TW; q += kPencilThreads) {
       const int s = q / TW, f = q - s * TW;
       if (f < tw_n) a.T[fb + (long)s * P + m * Lf + f0 + f] = tile[q];
+    }
+  }
+  if constexpr (MODE == PEN_QBQ_CG) {
+    // <p, Ap> for A = Q_r^* B^-1 Q_r: Q_r^* is N times the adjoint of Q_r (unnormalised
+    // forward DFT against the 1/N-scaled inverse), so <p, Ap> = N ||B^-1/2 Q_r p||^2 =
+    // (1/N) sum_e |IDFT(Pi p)_e|^2 / eps_e.  It is real and positive: the CG step is
+    // a = ||r||^2 / <p, Ap> (CG.cu:57-63, with Zdotc(p, Ap) formed in the field domain).
+    double acc[1] = {(double)dot};
+    __shared__ double sred[32];
+    block_reduce<1>(acc, sred);
+    const int nblk = gridDim.x * gridDim.y;  // CTAs of this slot (vec_per_slot == 1 in solves)
+    double tot[1];
+    if (slot_reduce<1>(acc, a.partials + (size_t)slot * nblk, a.counters + slot, blockIdx.y * gridDim.x + blockIdx.x,
+                       nblk, tot)) {
+      if (threadIdx.x == 0) {
+        CgState* st = a.cg + slot;
+        const double pAp = tot[0] / g.N;
+        st->a_re = pAp > 0 ? st->r1 / pAp : 0.0;
+        st->a_im = 0.0;
+        __threadfence();
+      }
     }
   }
 }
@@ -403,6 +462,21 @@ __global__ void __launch_bounds__(kPencilThreads, sizeof(R) == 4 ? 3 : 2) k_penc
 
 // ------------------------------------------------------------------ plane stage (forward)
 
+// End of a loop body in the forward plane stage: the last CTA of the grid decides
+// whether the loop (EPI_RESID: outer refinement, EPI_CGR: CG) runs again.  Every CTA,
+// live or not, arrives here once.
+template <int EPI, typename R>
+__device__ __forceinline__ void plane_fwd_decide(const PlaneOutArgs<R>& a) {
+  if (grid_last(a.counters + a.nslots, gridDim.x * gridDim.y * gridDim.z)) {
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int q = 0; q < a.nslots; q++)
+        any |= a.slots[q].active && (EPI == EPI_RESID ? a.cg[q].outer_active : a.cg[q].active);
+      decide_cond(a.cond, any);
+    }
+  }
+}
+
 template <typename R, bool GEN, int EPI, bool PR, int RARE, class GP>
 __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::kStatic ? (sizeof(R) == 4 ? 2 : 1) : (RARE >= 2 ? 1 : 2))
     k_plane_fwd(PlaneOutArgs<R> a) {
@@ -422,18 +496,10 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   const int slot = blockIdx.z;
   const Slot sl = a.slots[slot];
   bool live = sl.active;
-  if constexpr (EPI == EPI_CG) live = live && a.cg[slot].active;
+  if constexpr (EPI == EPI_CG || EPI == EPI_CGR) live = live && a.cg[slot].active;
   if constexpr (EPI == EPI_RESID) live = live && a.cg[slot].outer_active;
   if (!live) {
-    if constexpr (EPI == EPI_RESID) {
-      if (grid_last(a.counters + a.nslots, gridDim.x * gridDim.y * gridDim.z)) {
-        if (threadIdx.x == 0) {
-          int any = 0;
-          for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && a.cg[q].outer_active;
-          decide_cond(a.cond, any);
-        }
-      }
-    }
+    if constexpr (EPI == EPI_RESID || EPI == EPI_CGR) plane_fwd_decide<EPI>(a);
     return;
   }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
@@ -453,7 +519,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   }
   cp_async_wait_all();
   __syncthreads();
-  // forward 2-D transform.  General lattices (T*, FAME_FFT_CUDA.cu:297-319):
+  // forward 2-D transform.  General lattices (T*, FAME_FFT_CUDA.cu:128-150):
   // x conj(D_ky), y (mid) pass, x conj(D_kz), z (fast) pass.  Simple lattices:
   // fast then mid axis, no twiddles.
   for (int ax = 0; ax < 2; ax++) {
@@ -478,38 +544,102 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   const int Nd = sl.Nd, off = sl.off;
   const long vb = (long)(slot * a.vec_per_slot + vec) * a.vstride;
   double acc[2] = {0.0, 0.0};
-  for (int e = e0 + threadIdx.x; e < e1; e += GP::plane_threads()) {
-    const int fi = s * P + e;
-    if (fi < off) continue;
-    const long i = fi - off;
-    const int m = e / Lf, f = e - m * Lf;
-    const int q = m * S + f;
-    const cplx<R> t0 = src[0][q], t1 = src[1][q], t2 = src[2][q];
-    cplx<R> Lx, Ly, Lz;
-    lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
-    cplx<R> Pc[6];
-    pi_from<R>(GEN, PR, Lx, Ly, Lz, Pc);
-    const cplx<R> o1 = cadd(cadd(cmulc(Pc[0], t0), cmulc(Pc[1], t1)), cmulc(Pc[2], t2));
-    const cplx<R> o2 = cadd(cadd(cmulc(Pc[3], t0), cmulc(Pc[4], t1)), cmulc(Pc[5], t2));
-    if constexpr (EPI == EPI_OUT) {
-      a.out[vb + i] = o1;
-      a.out[vb + Nd + i] = o2;
-    } else if constexpr (EPI == EPI_CG) {
-      a.out[vb + i] = o1;
-      a.out[vb + Nd + i] = o2;
-      const cplx<R> p1 = a.p[vb + i], p2 = a.p[vb + Nd + i];
-      const cplx<R> d = cadd(cmulc(p1, o1), cmulc(p2, o2));  // conj(p) Ap
-      acc[0] += (double)d.x;
-      acc[1] += (double)d.y;
-    } else {  // EPI_RESID
-      const cplx<R> r1 = csub(a.b[vb + i], o1), r2 = csub(a.b[vb + Nd + i], o2);
-      a.out[vb + i] = r1;
-      a.out[vb + Nd + i] = r2;
-      acc[0] += (double)(cabs2(r1) + cabs2(r2));
+  // 3 -> 2 unmix and the epilogue.  The three components (remote shared memory) and
+  // the vector operand of KB points per thread are read up front, so one latency of
+  // each kind covers KB points.
+  constexpr int KB = GP::kStatic ? 4 : 2;
+  const int NT = GP::plane_threads();
+  R are = 0, aim = 0;
+  if constexpr (EPI == EPI_CGR) {
+    are = (R)a.cg[slot].a_re;
+    aim = (R)a.cg[slot].a_im;
+  }
+  for (int eb = e0 + threadIdx.x; eb < e1; eb += KB * NT) {
+    cplx<R> t[KB][3], va[KB], vb2[KB];
+#pragma unroll
+    for (int k = 0; k < KB; k++) {
+      const int e = eb + k * NT;
+      const int fi = s * P + e;
+      if (e < e1 && fi >= off) {
+        const long i = fi - off;
+        const int m = e / Lf, q = m * S + (e - m * Lf);
+#pragma unroll
+        for (int c = 0; c < 3; c++) t[k][c] = src[c][q];
+        if constexpr (EPI == EPI_CG) {
+          va[k] = a.p[vb + i];
+          vb2[k] = a.p[vb + Nd + i];
+        } else if constexpr (EPI == EPI_RESID) {
+          va[k] = a.b[vb + i];
+          vb2[k] = a.b[vb + Nd + i];
+        } else if constexpr (EPI == EPI_CGR) {
+          va[k] = a.r[vb + i];
+          vb2[k] = a.r[vb + Nd + i];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KB; k++) {
+      const int e = eb + k * NT;
+      const int fi = s * P + e;
+      if (e >= e1 || fi < off) continue;
+      const long i = fi - off;
+      const int m = e / Lf, f = e - m * Lf;
+      cplx<R> Lx, Ly, Lz;
+      lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
+      cplx<R> Pc[6];
+      pi_from<R>(GEN, PR, Lx, Ly, Lz, Pc);
+      const cplx<R> t0 = t[k][0], t1 = t[k][1], t2 = t[k][2];
+      const cplx<R> o1 = cadd(cadd(cmulc(Pc[0], t0), cmulc(Pc[1], t1)), cmulc(Pc[2], t2));
+      const cplx<R> o2 = cadd(cadd(cmulc(Pc[3], t0), cmulc(Pc[4], t1)), cmulc(Pc[5], t2));
+      if constexpr (EPI == EPI_OUT) {
+        a.out[vb + i] = o1;
+        a.out[vb + Nd + i] = o2;
+      } else if constexpr (EPI == EPI_CG) {
+        a.out[vb + i] = o1;
+        a.out[vb + Nd + i] = o2;
+        const cplx<R> d = cadd(cmulc(va[k], o1), cmulc(vb2[k], o2));  // conj(p) Ap
+        acc[0] += (double)d.x;
+        acc[1] += (double)d.y;
+      } else if constexpr (EPI == EPI_RESID) {
+        const cplx<R> r1 = csub(va[k], o1), r2 = csub(vb2[k], o2);
+        a.out[vb + i] = r1;
+        a.out[vb + Nd + i] = r2;
+        acc[0] += (double)(cabs2(r1) + cabs2(r2));
+      } else {  // EPI_CGR: r -= a Ap and ||r||^2 (CG.cu:71-76); Ap is never stored
+        cplx<R> r1 = va[k], r2 = vb2[k];
+        r1.x -= are * o1.x - aim * o1.y;
+        r1.y -= are * o1.y + aim * o1.x;
+        r2.x -= are * o2.x - aim * o2.y;
+        r2.y -= are * o2.y + aim * o2.x;
+        a.r[vb + i] = r1;
+        a.r[vb + Nd + i] = r2;
+        acc[0] += (double)(cabs2(r1) + cabs2(r2));
+      }
     }
   }
   cl.sync();  // remote shared memory must outlive the readers
 
+  if constexpr (EPI == EPI_CGR) {
+    __shared__ double sred[32];
+    double acc1[1] = {acc[0]};
+    block_reduce<1>(acc1, sred);
+    const int nblk = gridDim.x;  // CTAs of this slot (vec_per_slot == 1 in solves)
+    double tot[1];
+    if (slot_reduce<1>(acc1, a.partials + (size_t)slot * nblk, a.counters + slot, blockIdx.x, nblk, tot)) {
+      if (threadIdx.x == 0) {
+        // r0 = r1, r1 = <r, r>, k++ and the loop test r1 > tol^2 && k <= maxit (CG.cu:37, :73-77)
+        CgState* st = a.cg + slot;
+        st->r0 = st->r1;
+        st->r1 = tot[0];
+        st->beta = st->r1 / st->r0;
+        st->iter++;
+        st->total++;
+        st->active = (st->r1 > st->tol2) && (st->iter <= st->maxit);
+        __threadfence();
+      }
+    }
+    plane_fwd_decide<EPI>(a);
+  }
   if constexpr (EPI == EPI_CG || EPI == EPI_RESID) {
     __shared__ double sred[2 * 32];
     block_reduce<2>(acc, sred);
@@ -520,7 +650,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       if (threadIdx.x == 0) {
         CgState* st = a.cg + slot;
         if constexpr (EPI == EPI_CG) {
-          // a = r1 / dot  (CG.cu:325-328)
+          // a = r1 / dot  (CG.cu:60-63)
           const double den = tot[0] * tot[0] + tot[1] * tot[1];
           st->a_re = st->r1 * tot[0] / den;
           st->a_im = -st->r1 * tot[1] / den;
@@ -534,15 +664,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
         __threadfence();
       }
     }
-    if constexpr (EPI == EPI_RESID) {
-      if (grid_last(a.counters + a.nslots, gridDim.x * gridDim.y * gridDim.z)) {
-        if (threadIdx.x == 0) {
-          int any = 0;
-          for (int q = 0; q < a.nslots; q++) any |= a.slots[q].active && a.cg[q].outer_active;
-          decide_cond(a.cond, any);
-        }
-      }
-    }
+    if constexpr (EPI == EPI_RESID) plane_fwd_decide<EPI>(a);
   }
 }
 

@@ -109,6 +109,7 @@ struct fame_ctx {
   int pipe_ctas64 = 0;  // resident k_pencil_pipe<double> CTAs on the device
   int rare = 0;         // fft_lines level the axis plans need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
+  int loop_cap = 0;     // fame_set_loop_cap: bound on every device loop's trips (0: defaults)
   bool have_eps = false;
   // persistent data
   DBuf<double2> tw64;
@@ -132,7 +133,7 @@ struct fame_ctx {
   DBuf<unsigned> counters, tri_ctr;
   DBuf<int> map, prof, status, flags;
   DBuf<double2> U, r64, x64, b64, p64, Ap64, T64, EV, AV, Tb, E;
-  DBuf<float2> r32, x32, p32, Ap32, T32;
+  DBuf<float2> r32, x32, p32, T32;
   int* hflag = nullptr;  // pinned
   // recorded programs keyed by configuration
   std::map<std::string, std::unique_ptr<Program>> progs;
@@ -249,11 +250,13 @@ struct Ops {
     a.vec_per_slot = nvec;
     a.T = T;
     a.invB = invB;
-    a.ib_field = MODE == PEN_QBQ ? 1 : 0;
+    a.ib_field = MODE == PEN_QBQ || MODE == PEN_QBQ_CG ? 1 : 0;
     a.out = out;
     a.in = in;
     a.cg = c->cg.p;
     a.gate = gate;
+    a.partials = c->partials.p;
+    a.counters = c->counters.p;
     a.TW = pencil_tw<R>();
     a.nslots = nslots;
     const size_t sm = pencil_smem<R>(g());
@@ -290,8 +293,9 @@ struct Ops {
   template <typename R, int EPI, bool PR>
   void plane_fwd(const cplx<R>* T, cplx<R>* out, int nvec, long vstride, long fstride,
                  const cplx<R>* p = nullptr, const cplx<R>* b = nullptr, Cond cond = Cond{},
-                 double tol2 = 0) {
+                 double tol2 = 0, cplx<R>* r = nullptr) {
     PlaneOutArgs<R> a;
+    a.r = r;
     a.g = g();
     a.slots = c->slots.p;
     a.tabs = c->tabs.p;
@@ -504,7 +508,6 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
     c->r32.ensure((size_t)nslots * M);
     c->x32.ensure((size_t)nslots * M);
     c->p32.ensure((size_t)nslots * M);
-    c->Ap32.ensure((size_t)nslots * M);
     c->T32.ensure((size_t)nslots * 3 * N);
   }
   // FP64 CG vectors: every context may run FP64 solves and A_r^-1 applies, whatever
@@ -601,15 +604,16 @@ __global__ void __launch_bounds__(256) k_adj_grad(const double2* E, const double
 // ------------------------------------------------------------------ recording
 struct SolveCfg {
   int nslots, nstep, nwant, es_maxit, ls_maxit, mixed, vec, inner_maxit;
-  int enorm;  // restore E (norms only) for the reference-scaled residual
+  int enorm;     // restore E (norms only) for the reference-scaled residual
+  int loop_cap;  // bound on every device loop's trips (0: the defaults)
   double es_tol, ls_tol, inner_tol;
 };
 
 static std::string cfg_key(const SolveCfg& s, bool graph) {
   char b[256];
-  snprintf(b, sizeof b, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%.17g/%.17g/%.17g/%d", s.nslots, s.nstep, s.nwant,
+  snprintf(b, sizeof b, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%.17g/%.17g/%.17g/%d/%d", s.nslots, s.nstep, s.nwant,
            s.es_maxit, s.ls_maxit, s.mixed, s.vec, s.enorm, s.inner_maxit, s.es_tol, s.ls_tol, s.inner_tol,
-           (int)graph);
+           (int)graph, s.loop_cap);
   return b;
 }
 
@@ -618,8 +622,8 @@ static std::string cfg_key(const SolveCfg& s, bool graph) {
 // device ints of the loop conditions: flag of loop i at flags[i], its trip counter
 // and overflow marker at flags[kTrips + 2i]
 constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopNone = 3, kLoopRestart = 4, kTrips = 32;
-static Cond loop_cond(Program& P, int* flags, int id, int cap) {
-  return P.make_cond(flags + id, flags + kTrips + 2 * id, cap);
+static Cond loop_cond(Program& P, int* flags, int id, int cap, int loop_cap = 0) {
+  return P.make_cond(flags + id, flags + kTrips + 2 * id, loop_cap > 0 ? std::min(cap, loop_cap) : cap);
 }
 
 static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base) {
@@ -631,7 +635,7 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
   const long F = 3L * g.N;
   const double tol2 = s.ls_tol * s.ls_tol;
   if (!s.mixed) {
-    Cond cc = loop_cond(P, flag_base, kLoopCG, s.ls_maxit + 2);
+    Cond cc = loop_cond(P, flag_base, kLoopCG, s.ls_maxit + 2, s.loop_cap);
     P.launch(k_invar_pro<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(cc), L, j, c->r64.p, c->x64.p,
              (double2*)nullptr, tol2, s.ls_maxit);
     P.while_loop(cc, [&] {
@@ -645,20 +649,21 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
     P.launch(k_invar_epi<false>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L, j,
              (const double2*)c->x64.p, (const double2*)c->p64.p);
   } else {
-    Cond outer = loop_cond(P, flag_base, kLoopOuter, 42);
-    Cond inner = loop_cond(P, flag_base, kLoopInner, s.inner_maxit + 2);
+    Cond outer = loop_cond(P, flag_base, kLoopOuter, 42, s.loop_cap);
+    Cond inner = loop_cond(P, flag_base, kLoopInner, s.inner_maxit + 2, s.loop_cap);
     P.launch(k_invar_pro<true>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(outer), L, j, c->r64.p, c->x64.p,
              c->b64.p, tol2, s.ls_maxit);
     P.while_loop(outer, [&] {
       P.launch(k_cg32_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), (const double2*)c->r64.p,
                c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit, tol2, outer);
+      // FP32 CG, three kernels per iteration: p and the deferred x update with the
+      // 2 -> 3 mix; the slow-axis transforms with <p, Ap>; the 3 -> 2 unmix with
+      // r -= a Ap, ||r||^2 and the loop decision (Ap is never stored)
       P.while_loop(inner, [&] {
         o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr,
                                          inner, c->x32.p);
-        o.pencil<float, PEN_QBQ>(c->T32.p, 1, F, c->ibq32(), 1);
-        o.plane_fwd<float, EPI_CG, false>(c->T32.p, c->Ap32.p, 1, M, F, c->p32.p);
-        P.launch(k_cg_update<float>, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), c->r32.p,
-                 (const float2*)c->Ap32.p);
+        o.pencil<float, PEN_QBQ_CG>(c->T32.p, 1, F, c->ibq32(), 1);
+        o.plane_fwd<float, EPI_CGR, false>(c->T32.p, nullptr, 1, M, F, nullptr, nullptr, inner, 0.0, c->r32.p);
       });
       o.plane_inv<double, IN_REFINE, false>(nullptr, c->T64.p, 1, M, F, 0, nullptr, nullptr, c->x64.p,
                                             c->x32.p, Cond{}, nullptr, c->p32.p);
@@ -692,13 +697,14 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
   L.h = c->hcoef.p;
   L.lz = c->lz.p;
   L.prof = c->prof.p;
+  L.status = c->status.p;
   int* flags = c->flags.p;
   const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
   P.launch(k_tables, dim3((tmax + 255) / 256, s.nslots), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
            (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
   P.launch(k_lz_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(Cond{}), L);
   for (int j = 0; j < s.nstep; j++) emit_step(o, s, L, j, flags);
-  Cond restart = loop_cond(P, flags, kLoopRestart, s.es_maxit + 2);
+  Cond restart = loop_cond(P, flags, kLoopRestart, s.es_maxit + 2, s.loop_cap);
   TriArgs ta;
   ta.L = L;
   ta.slots = c->slots.p;
@@ -752,7 +758,7 @@ static double slot_bytes(const fame_ctx* c, int nstep, int nwant, bool mixed, bo
              + 2 * M * z + 3 * N * z           // r64, x64, T64
              + 2 * nwant * M * z + nwant * 3 * N * z  // EV, AV, Tb
              + 2 * M * z;                      // p64, Ap64
-  if (mixed) b += M * z + 4 * M * 8 + 3 * N * 8;  // b64, r32, x32, p32, Ap32, T32
+  if (mixed) b += M * z + 3 * M * 8 + 3 * N * 8;  // b64, r32, x32, p32, T32
   if (vec) b += nwant * 3 * N * z;               // E
   return b;
 }
@@ -830,7 +836,7 @@ void fame_ctx_destroy(fame_ctx* c) {
   for (auto* b : {&c->tw64, &c->tabs, &c->U, &c->r64, &c->x64, &c->b64, &c->p64, &c->Ap64, &c->T64, &c->EV,
                   &c->AV, &c->Tb, &c->E})
     b->release();
-  for (auto* b : {&c->r32, &c->x32, &c->p32, &c->Ap32, &c->T32, &c->tw32}) b->release();
+  for (auto* b : {&c->r32, &c->x32, &c->p32, &c->T32, &c->tw32}) b->release();
   for (auto* b : {&c->invB64, &c->invB64q, &c->B64, &c->partials, &c->T0, &c->T1, &c->hcoef, &c->theta, &c->Z, &c->G,
                   &c->stats})
     b->release();
@@ -940,6 +946,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     return FAME_ERR_BAD_INPUT;
   }
   int rc_all = FAME_OK;
+  int status_any = 0;
   try {
     FAME_CK(cudaSetDevice(c->device));
     SolveCfg s;
@@ -955,6 +962,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     s.ls_tol = p.ls_tol;
     s.inner_tol = p.inner_tol > 0 ? p.inner_tol : 2e-6;  // two FP64 refinement steps reach 1e-12
     s.inner_maxit = p.inner_maxit > 0 ? p.inner_maxit : 200;
+    s.loop_cap = c->loop_cap;
     const bool graph = p.use_graph != 0;
     ensure_workspace(c, s.nslots, s.nstep, s.nwant, s.mixed, s.vec || s.enorm);
     const std::string key = cfg_key(s, graph);
@@ -1060,10 +1068,12 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
           kc.es_iter = prof[3 * q + 1];
           kc.restarts = lz[q].restarts;
           kc.status = status[q] == 0 ? FAME_OK : FAME_ERR_NO_CONVERGENCE;
+          kc.detail = status[q];
           kc.Nd = hs[q].Nd;
           kc.refine = prof[3 * q + 2];
         }
         if (status[q] != 0) rc_all = FAME_ERR_NO_CONVERGENCE;
+        status_any |= status[q];
         if (s.vec) {
           const size_t n3 = 3 * (size_t)N;
           double2* dst = reinterpret_cast<double2*>(evec_out) + (size_t)kk * s.nwant * n3;
@@ -1086,7 +1096,13 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     set_err(e.what());
     return FAME_ERR_WATCHDOG;
   }
-  if (rc_all) set_err("Lanczos did not converge within es_maxit restarts for some k-point");
+  if (rc_all) {
+    std::string m = "no convergence for some k-point:";
+    if (status_any & kStatusCG) m += " an A_r^-1 solve stopped above ls_tol (ls_maxit or the refinement cap);";
+    if (status_any & kStatusLanczos) m += " Lanczos did not converge within es_maxit restarts;";
+    if (status_any & kStatusQL) m += " the tridiagonal eigensolve failed;";
+    set_err(m);
+  }
   return rc_all;
 }
 
@@ -1165,6 +1181,7 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
           L.h = c->hcoef.p;
           L.lz = c->lz.p;
           L.prof = c->prof.p;
+          L.status = c->status.p;
           P.launch(k_lz_init, dim3(1, 1, 1), dim3(256), 0, o.va(Cond{}), L);
           FAME_CK(cudaMemcpyAsync(c->U.p, x, 2L * sl.Nd * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
           SolveCfg s;
@@ -1230,6 +1247,15 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
 }
 
 void* fame_ctx_stream(fame_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int fame_set_loop_cap(fame_ctx* c, int max_trips) {
+  if (!c || max_trips < 0) {
+    set_err("null context or negative loop cap");
+    return FAME_ERR_BAD_INPUT;
+  }
+  c->loop_cap = max_trips;
+  return FAME_OK;
+}
 
 int fame_launch_count(fame_ctx* c, unsigned long long* out) {
   if (!c || !out) {

@@ -73,7 +73,7 @@ struct VecArgs {
 };
 
 // ---------------------------------------------------------------- CG update
-// x += a p ; r -= a Ap ; r1 = <r, r>  (FAME_Main/CG.cu:330-341); then beta, the
+// x += a p ; r -= a Ap ; r1 = <r, r>  (FAME_Main/CG.cu:65-76); then beta, the
 // iteration counter and the loop test r1 > tol^2 && k <= maxit (:302).
 template <typename R>
 __global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* r, const cplx<R>* Ap) {
@@ -135,7 +135,14 @@ struct LzArgs {
   double* h;               // [nslots][nstep+2] reorthogonalisation coefficients
   LzState* lz;
   int* prof;               // [nslots][3]: ls_iter, es_iter (reference Profile counters), FP64 refinements
+  int* status;             // [nslots] per-k status bits (kStatus*)
 };
+
+// Per-k status bits: the tridiagonal QL iteration failed; Lanczos ended at es_maxit
+// restarts unconverged (Lanczos_Isotropic.cu:84-85 prints this case); an A_r^-1 solve
+// ended at ls_maxit (plain) or at the refinement cap (mixed) above ls_tol (CG.cu:81-84
+// prints this case).  The host reports any of them as FAME_ERR_NO_CONVERGENCE.
+constexpr int kStatusQL = 1, kStatusLanczos = 2, kStatusCG = 4;
 
 __device__ __forceinline__ double2* ucol(const LzArgs& L, int slot, int logical) {
   const int ph = L.map[slot * (L.nstep + 1) + logical];
@@ -180,6 +187,7 @@ __global__ void __launch_bounds__(256) k_invar_pro(VecArgs va, LzArgs L, int j, 
           st->active = (tot[0] > tol2) && (1 <= maxit);
         } else {
           st->rr = tot[0];
+          st->otol2 = tol2;
           st->scale = 1.0 / sqrt(tot[0] > 0 ? tot[0] : 1.0);
           st->outer = 0;
           st->outer_max = 40;  // refinement steps per solve; each gains ~5 digits
@@ -260,7 +268,7 @@ __global__ void __launch_bounds__(256) k_cg32_init(VecArgs va, const double2* r6
 }
 
 // invAr epilogue: w = x / sqrt(Lambda_q) into U[:, j+1] (…invAr.cu:45) and
-// alpha_j = Re<w, u_j> (Lanczos_decomp_gpu.cu:307-309); profile counters
+// alpha_j = Re<w, u_j> (Lanczos_decomp_gpu.cu:64-66); profile counters
 // (…invAr.cu:41-43: ls_iter += k, es_iter++).
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, const double2* x64,
@@ -303,6 +311,7 @@ __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, 
       L.prof[slot * 3 + 0] += MIXED ? st->total : st->iter;
       L.prof[slot * 3 + 1] += 1;
       if (MIXED) L.prof[slot * 3 + 2] += st->outer_total;
+      if (MIXED ? st->rr > st->otol2 : st->r1 > st->tol2) L.status[slot] |= kStatusCG;
     }
   }
 }
@@ -311,7 +320,7 @@ __global__ void __launch_bounds__(256) k_invar_epi(VecArgs va, LzArgs L, int j, 
 // w' = w - alpha_j u_j - beta_{j-1} u_{j-1}; ||w'||^2 and, for j >= 1, the
 // coefficients <u_i, w'> (i <= j) of one classical Gram-Schmidt pass.  The
 // reference normalises first and then runs one modified Gram-Schmidt pass
-// without renormalising (Lanczos_decomp_gpu.cu:311-329); both leave u_{j+1}
+// without renormalising (Lanczos_decomp_gpu.cu:68-87); both leave u_{j+1}
 // orthogonal to the basis to rounding level.
 constexpr int kLzRows = 2048;  // rows per CTA, staged in shared memory (32 KB)
 
@@ -490,7 +499,7 @@ struct TriArgs {
   int maxit;
   Cond cond;       // "some slot needs another restart"
   int nslots;
-  int* status;     // [nslots] 0 ok, 2 no convergence, 3 QL failure
+  int* status;     // [nslots] bits: kStatusQL, kStatusLanczos, kStatusCG (0: converged)
   unsigned* ctr;   // grid ticket counter
   int first;       // 1: the call before the restart loop (starts it), 0: end of a loop body
 };
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(32) k_tridiag(TriArgs a) {
         else break;
       }
       lz->nconv = conv;
-      if (fail) a.status[slot] = 3;
+      if (fail) a.status[slot] |= kStatusQL;
     }
     conv = __shfl_sync(0xffffffffu, conv, 0);
     const bool done = conv == nw || fail;
@@ -651,7 +660,7 @@ __global__ void __launch_bounds__(32) k_tridiag(TriArgs a) {
     } else if (lz->restarts >= a.maxit) {
       if (lane == 0) {
         lz->converged = 1;
-        a.status[slot] = 2;
+        a.status[slot] |= kStatusLanczos;
       }
     } else {
       // ---- lock & purge on G (order nstep+1)

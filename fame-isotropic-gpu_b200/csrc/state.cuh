@@ -17,12 +17,13 @@ struct CgState {
   double r1, r0, beta;       // ||r||^2 now / before, r1/r0
   double a_re, a_im;         // CG step a = r1 / <p, Ap>
   double r1_0, tol2;         // initial ||r||^2, stop threshold on ||r||^2
-  int iter;                  // the reference's counter k (starts at 1, CG.cu:301)
+  int iter;                  // the reference's counter k (starts at 1, CG.cu:36)
   int active;
   int maxit;
   int total;                 // CG products accumulated for the profile counter
   // outer iterative refinement (mixed precision)
   double rr, scale;          // ||b - A y||^2, 1/||b - A y|| used to scale the FP32 rhs
+  double otol2;              // stop threshold of the refinement on ||b - A y||^2 (ls_tol^2)
   int outer, outer_active, outer_max, outer_total;
 };
 
@@ -99,8 +100,11 @@ __device__ __forceinline__ cplx<R> dkz_at(const Geom& g, const double2* tab, int
 
 // ------------------------------------------------------------------ plane stage
 enum InMode { IN_VEC = 0, IN_CG = 1, IN_REFINE = 2 };
-enum EpiMode { EPI_OUT = 0, EPI_CG = 1, EPI_RESID = 2 };
-enum PencilMode { PEN_QBQ = 0, PEN_QR_OUT = 1, PEN_QRS_IN = 2 };
+// EPI_CG writes Ap and forms <p, Ap>; EPI_CGR (fused CG) keeps Ap in registers and
+// applies r -= a Ap with ||r||^2, the step size a coming from the PEN_QBQ_CG pencil.
+enum EpiMode { EPI_OUT = 0, EPI_CG = 1, EPI_RESID = 2, EPI_CGR = 3 };
+// PEN_QBQ_CG: PEN_QBQ that also reduces <p, Ap> = (1/N) sum_e |(IDFT v)_e|^2 / eps_e
+enum PencilMode { PEN_QBQ = 0, PEN_QR_OUT = 1, PEN_QRS_IN = 2, PEN_QBQ_CG = 3 };
 
 template <typename R>
 struct PlaneInArgs {
@@ -137,8 +141,10 @@ struct PencilArgs {
   int ib_field;            // invB in the field layout (else the spatial layout; same for Simple lattices)
   cplx<R>* out;            // PEN_QR_OUT: spatial field out (3N per vector)
   const cplx<R>* in;       // PEN_QRS_IN: spatial field in
-  const CgState* cg;       // optional activity gate
+  CgState* cg;             // optional activity gate; PEN_QBQ_CG writes the step size a
   int gate;                // 0 none, 1 CG active, 2 outer refinement active
+  double* partials;        // PEN_QBQ_CG: [nslots][CTAs per slot] partial sums
+  unsigned* counters;      // PEN_QBQ_CG: [nslots] ticket counters
   int TW;                  // fast positions per CTA
   int nslots;              // k-points of the launch (k_pencil_pipe walks all their tiles)
 };
@@ -154,11 +160,12 @@ struct PlaneOutArgs {
   const cplx<R>* T;        // field after the slow-axis forward pass
   cplx<R>* out;            // EPI_OUT: reduced output; EPI_CG: Ap; EPI_RESID: r (FP64)
   const cplx<R>* p;        // EPI_CG: p for <p, Ap>
+  cplx<R>* r;              // EPI_CGR: CG residual, updated in place
   const cplx<R>* b;        // EPI_RESID: right-hand side
   CgState* cg;
   double* partials;        // [nslots][blocks per slot][NV]
   unsigned* counters;      // [nslots] ticket counters, plus [nslots] = grid counter
-  Cond cond;               // EPI_RESID: outer WHILE condition
+  Cond cond;               // EPI_RESID: outer WHILE condition; EPI_CGR: CG WHILE condition
   int nslots;
   double tol2;             // EPI_RESID: absolute tolerance^2 on ||b - A y||
 };

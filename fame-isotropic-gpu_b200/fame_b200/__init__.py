@@ -30,7 +30,9 @@ OP_QR, OP_QRS, OP_QBQ, OP_PR, OP_PRS, OP_INVAR = range(6)
 EXPORTS = ("fame_ctx_create", "fame_ctx_destroy", "fame_set_eps", "fame_set_material", "fame_solve_kpoints",
            "fame_apply", "fame_adjoint", "fame_ctx_sizes", "fame_last_error", "fame_version", "fame_ctx_stream",
            "fame_launch_count", "fame_bench_qbq", "fame_qbq_static", "fame_material_locate",
-           "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish")
+           "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish", "fame_set_loop_cap")
+# fame_kcounters.detail bits (FAME_KSTATUS_*)
+KSTATUS_QL, KSTATUS_LANCZOS, KSTATUS_CG = 1, 2, 4
 QBQ_STATIC_SCRATCH_BYTES = 4 << 20  # FAME_QBQ_STATIC_SCRATCH_BYTES
 
 
@@ -66,7 +68,7 @@ class MaterialShapes(C.Structure):
 
 class KCounters(C.Structure):
     _fields_ = [("ls_iter", C.c_int), ("es_iter", C.c_int), ("restarts", C.c_int), ("status", C.c_int),
-                ("Nd", C.c_int), ("refine", C.c_int)]
+                ("Nd", C.c_int), ("refine", C.c_int), ("detail", C.c_int)]
 
 
 _lib = None
@@ -101,11 +103,13 @@ def load():
     lib.fame_write_eigenvectors.argtypes = [C.c_char_p, D, C.c_int, C.c_longlong, C.c_int, C.c_int]
     lib.fame_writer_start.argtypes = [C.c_char_p, D, C.c_int, C.c_longlong, C.c_int, C.c_int, C.POINTER(P)]
     lib.fame_writer_finish.argtypes = [P]
+    lib.fame_set_loop_cap.argtypes = [P, C.c_int]
     lib.fame_last_error.restype = C.c_char_p
     lib.fame_version.restype = C.c_char_p
     for fn in ("fame_ctx_create", "fame_set_eps", "fame_set_material", "fame_solve_kpoints", "fame_apply",
                "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq", "fame_qbq_static",
-               "fame_material_locate", "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish"):
+               "fame_material_locate", "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish",
+               "fame_set_loop_cap"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib
@@ -118,6 +122,39 @@ def _check(rc):
 
 def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def reduced_size(lattice, k):
+    """Nd of wave vector k on `lattice` (a Lattice): N - 1 at the Gamma point (|k| below
+    1e-4 for Simple lattices, 1e-3 for General ones, FAME_Main/FAME_Matrix_Lambdas.cu:157
+    and :406), else N.  The same rule as the library's."""
+    N = int(lattice.grid[0]) * int(lattice.grid[1]) * int(lattice.grid[2])
+    kk = np.asarray(k, dtype=np.float64).reshape(-1)
+    if kk.size != 3:
+        raise ValueError("k must have 3 components")
+    return N - 1 if float(np.sqrt(np.sum(kk * kk))) < (1e-4 if lattice.simple else 1e-3) else N
+
+
+def _check_device_tensor(t, name, dtype, numel, device):
+    """Raises ValueError unless t is a contiguous CUDA tensor of `dtype` with exactly
+    `numel` elements on CUDA device `device` (None: the current device): the library
+    reads and writes exactly that many elements at t.data_ptr(), so anything else
+    would run out of bounds."""
+    import torch
+    if not isinstance(t, torch.Tensor):
+        raise ValueError(f"{name} must be a torch tensor")
+    if t.device.type != "cuda":
+        raise ValueError(f"{name} must be a CUDA tensor (got {t.device})")
+    if device is None:
+        device = torch.cuda.current_device()
+    if t.device.index != device:
+        raise ValueError(f"{name} must be on cuda:{device} (got {t.device})")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype} (got {t.dtype})")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if t.numel() != numel:
+        raise ValueError(f"{name} must have {numel} elements (got {t.numel()})")
 
 
 def make_lattice(grid, mesh_len, lattice_vec_a, simple, m=(0, 0, 0, 0), t1=(0.0, 0.0, 0.0)):
@@ -147,6 +184,7 @@ class Context:
         lib = load()
         self._lat = make_lattice(grid, mesh_len, lattice_vec_a, simple, m, t1)
         self.N = int(np.prod(grid))
+        self.device = int(device)
         h = C.c_void_p()
         _check(lib.fame_ctx_create(device, C.byref(self._lat), C.byref(h)))
         self._h = h
@@ -194,7 +232,7 @@ class Context:
                                        ev.ctypes.data_as(C.POINTER(C.c_double)) if ev is not None else None, cnt)
         out = dict(freq=freq, relres=rr, relerr=re, rc=rc,
                    counters=[dict(ls_iter=c.ls_iter, es_iter=c.es_iter, restarts=c.restarts, status=c.status,
-                                  Nd=c.Nd, refine=c.refine) for c in cnt])
+                                  Nd=c.Nd, refine=c.refine, detail=c.detail) for c in cnt])
         if ev is not None:
             out["evec"] = ev
         if ra is not None:
@@ -204,14 +242,28 @@ class Context:
         return out
 
     def apply(self, op, k, x, y, precision=FP64, params=None):
-        """Applies operator `op` at wave vector k to device buffers x -> y (torch CUDA
-        tensors, complex128 for FP64 / complex64 for MIXED).  Returns Nd."""
+        """Applies operator `op` at wave vector k to device buffers x -> y (contiguous
+        torch CUDA tensors on the context's device, complex128 for FP64 / complex64 for
+        MIXED; reduced vectors have 2*Nd elements, fields 3N).  Returns Nd.  Raises
+        ValueError on a tensor of the wrong device, type, layout or size."""
+        import torch
         kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+        Nd = reduced_size(self._lat, kk)
+        dt = torch.complex128 if precision == FP64 else torch.complex64
+        n_in = 3 * self.N if op in (OP_QRS, OP_PRS) else 2 * Nd
+        n_out = 3 * self.N if op in (OP_QR, OP_PR) else 2 * Nd
+        _check_device_tensor(x, "x", dt, n_in, self.device)
+        _check_device_tensor(y, "y", dt, n_out, self.device)
         nd = C.c_int()
         p = params or solver_params()
         _check(load().fame_apply(self._h, int(op), _dptr(kk), C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                                  int(precision), C.byref(p), C.byref(nd)))
         return nd.value
+
+    def set_loop_cap(self, max_trips):
+        """Bounds every device loop of later solves to max_trips trips (0: defaults);
+        a loop that reaches it ends the solve with ERR_WATCHDOG."""
+        _check(load().fame_set_loop_cap(self._h, int(max_trips)))
 
     def stream(self):
         """The context's cudaStream_t as an int (for torch.cuda.ExternalStream)."""
@@ -277,9 +329,17 @@ def material_locate(grid, mesh_len, lattice_vec_a, Omega, permutation, material,
 def qbq_static(lattice, k, inv_b, x, y, stream=0):
     """Q_r^* B^-1 Q_r in FP64 through fame_qbq_static (no device allocation, no
     context): lattice from make_lattice, inv_b (3N float64), x and y (2*Nd
-    complex128) torch CUDA tensors; enqueued on `stream` (a cudaStream_t as int,
-    0 = legacy default stream), not synchronised."""
+    complex128) contiguous torch CUDA tensors on the current device; enqueued on
+    `stream` (a cudaStream_t as int, 0 = legacy default stream), not synchronised.
+    Raises ValueError on a tensor of the wrong device, type, layout or size."""
+    import torch
     kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+    N = int(lattice.grid[0]) * int(lattice.grid[1]) * int(lattice.grid[2])
+    Nd = reduced_size(lattice, kk)
+    # the call runs on the current device (whose scratch array it uses)
+    _check_device_tensor(inv_b, "inv_b", torch.float64, 3 * N, None)
+    _check_device_tensor(x, "x", torch.complex128, 2 * Nd, None)
+    _check_device_tensor(y, "y", torch.complex128, 2 * Nd, None)
     _check(load().fame_qbq_static(C.byref(lattice), _dptr(kk), C.c_void_p(inv_b.data_ptr()),
                                   C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(stream)))
 

@@ -86,6 +86,19 @@ int FAME_Main_Code(PAR Par, PROFILE* Profile) {
     fprintf(stderr, "FAME_Main_Code: material type %s is not supported\n", Par.material.material_type);
     return FAME_ERR_UNSUPPORTED;
   }
+  if (Par.material.num_ele_permitt_in < Par.material.material_num) {
+    // The reference prompts on stdin for the missing values here
+    // (FAME_Main/FAME_Matrix_B_Isotropic.cu:13-24); a library call must not, so the
+    // run ends with a status.  Binout and ele_permitt_in are released as the
+    // reference's FAME_Matrix_B_Isotropic releases them (:69-72).
+    fprintf(stderr,
+            "FAME_Main_Code: %d inner permittivities given for %d materials (Popt.txt "
+            "\"# Permittivity (inner material)\" needs one per material)\n",
+            Par.material.num_ele_permitt_in, Par.material.material_num);
+    free(Par.material.Binout);
+    free(Par.material.ele_permitt_in);
+    return FAME_ERR_BAD_INPUT;
+  }
   fame_ctx* ctx = nullptr;
   int rc = fame_ctx_create(Par.flag.device, &lat, &ctx);
   if (rc != FAME_OK) return fail(rc, "fame_ctx_create");

@@ -4,13 +4,13 @@
 # Popt.txt and the material description and writes Data_Omega_array.txt exactly as
 # the reference's Main.out does, with the band-structure solve on this library.
 #
-#   fame-isotropic-gpu_b200/shim/build_main.sh [REFERENCE_ROOT]   (default: /root/reference)
+#   fame-isotropic-gpu_b200/shim/build_main.sh REFERENCE_ROOT   (the reference project's root directory)
 #
 # The reference sources are compiled where they lie (none is copied or edited);
 # objects and the program go to fame-isotropic-gpu_b200/shim/_build/.  Run
 # `make -C fame-isotropic-gpu_b200` first.
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:?"usage: $0 REFERENCE_ROOT"}
 HERE=$(cd "$(dirname "$0")" && pwd)
 PKG=$(dirname "$HERE")
 OUT="$HERE/_build"

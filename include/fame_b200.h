@@ -80,13 +80,21 @@ typedef struct {
 /* Per k-point counters (the reference's PROFILE, include/FAME_Internal_Common.h:205-211,
  * plus the mixed-precision breakdown). */
 typedef struct {
-  int ls_iter;      /* Profile.ls_iter: CG products (reference counting, CG.cu:301,342) */
+  int ls_iter;      /* Profile.ls_iter: CG products (reference counting, CG.cu:36-77) */
   int es_iter;      /* Profile.es_iter: A_r^-1 applications */
   int restarts;     /* Lanczos restarts */
   int status;       /* FAME_OK / FAME_ERR_NO_CONVERGENCE for this k */
   int Nd;           /* N or N-1 (Gamma point) */
   int refine;       /* FAME_MIXED: FP64 refinement steps (each one FP64 Q_r^* B^-1 Q_r); else 0 */
+  int detail;       /* why status is FAME_ERR_NO_CONVERGENCE, FAME_KSTATUS_* bits (0 when FAME_OK) */
 } fame_kcounters;
+
+/* fame_kcounters.detail bits.  The reference only prints these cases
+ * (FAME_Main/CG.cu:81-84, FAME_Main/Lanczos_Isotropic.cu:84-85). */
+#define FAME_KSTATUS_QL 1      /* the tridiagonal eigensolve did not converge */
+#define FAME_KSTATUS_LANCZOS 2 /* Lanczos stopped at es_maxit restarts unconverged */
+#define FAME_KSTATUS_CG 4      /* an A_r^-1 solve stopped above ls_tol: ls_maxit products (FP64) or
+                                  the refinement cap (FAME_MIXED) */
 
 /* Create a context on `device` for one lattice/grid.  Allocates nothing per k yet. */
 int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out);
@@ -98,7 +106,7 @@ int fame_set_eps(fame_ctx* ctx, const double* B_eps);
 
 /* B from the reference's material index map Binout (3 * material_num * N ints,
  * FAME_Preprocessing/FAME_Material_Locate_Index.cpp:101-113) with the same
- * last-material-wins rule as FAME_Matrix_B_Isotropic.cu:100-131. */
+ * last-material-wins rule as FAME_Matrix_B_Isotropic.cu:41-61. */
 int fame_set_material(fame_ctx* ctx, const int* binout, int material_num, const double* eps_in,
                       double eps_out);
 
@@ -142,6 +150,14 @@ void* fame_ctx_stream(fame_ctx* ctx);
 /* Number of kernels of this library launched on the device so far (counted on the
  * device by every kernel's first thread, graph-launched kernels included). */
 int fame_launch_count(fame_ctx* ctx, unsigned long long* count_out);
+
+/* Bound on the trips of every device loop of later solves on this context: the CG,
+ * refinement, inner FP32 and Lanczos restart loops each stop after at most
+ * `max_trips` trips (0 restores the defaults: ls_maxit + 2, 42, inner_maxit + 2 and
+ * es_maxit + 2, which only a fault reaches).  A loop that reaches its bound ends the
+ * solve with FAME_ERR_WATCHDOG instead of running on.  No counterpart in the
+ * reference, whose loops are host-driven. */
+int fame_set_loop_cap(fame_ctx* ctx, int max_trips);
 
 /* Operator benchmark: `reps` applications of Q_r^* B^-1 Q_r at wave vector k in
  * FP64 (precision FAME_FP64) or FP32 (FAME_MIXED) to a batch of `nbatch` vectors

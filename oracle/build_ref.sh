@@ -3,7 +3,7 @@
 # lie, for sm_100a, into oracle/_ref/.  Test infrastructure only: the product
 # never links or runs anything built here.
 #
-#   oracle/build_ref.sh [REFERENCE_ROOT]      (default: /root/reference)
+#   oracle/build_ref.sh REFERENCE_ROOT      (the reference project's root directory)
 #
 # Outputs (git-ignored, they travel to the GPU box with the tree):
 #   oracle/_ref/fame_ref_main     the reference's own Main.cpp program
@@ -14,7 +14,7 @@
 # Only header shims are added (oracle/ref_shims/); no reference source is edited or
 # copied.  LAPACKE_zpteqr is bound to scipy's bundled OpenBLAS (LP64 LAPACKE).
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:?"usage: $0 REFERENCE_ROOT"}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"

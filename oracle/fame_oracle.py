@@ -174,7 +174,7 @@ def lambdas(wave_vec, par):
 
 # ------------------------------------------------------------------ transforms
 def _T_general(p, L: Lambdas):
-    """spMV_fastT_gpu flag=+1 on one component (FAME_FFT_CUDA.cu:272-294)."""
+    """spMV_fastT_gpu flag=+1 on one component (FAME_FFT_CUDA.cu:104-125)."""
     Nx, Ny, Nz = L.grid
     a = p.reshape(Nx, Ny, Nz)
     a = np.fft.ifft(a, axis=2) * Nz
@@ -187,7 +187,7 @@ def _T_general(p, L: Lambdas):
 
 
 def _Ts_general(v, L: Lambdas):
-    """spMV_fastT_gpu flag=-1 on one component (FAME_FFT_CUDA.cu:297-319)."""
+    """spMV_fastT_gpu flag=-1 on one component (FAME_FFT_CUDA.cu:128-150)."""
     Nx, Ny, Nz = L.grid
     a = v.reshape(Nz, Ny, Nx).transpose(2, 1, 0)
     a = a * np.conj(L.D_kx)[:, None, None]
@@ -281,7 +281,7 @@ def cg(apply, rhs, tol, maxit):
             p = r.copy()
         Ap = apply(p)
         dot = np.vdot(p, Ap)
-        a = r1 / dot  # = r1*conj(dot)/|dot|^2, CG.cu:326-328
+        a = r1 / dot  # = r1*conj(dot)/|dot|^2, CG.cu:60-63
         x = x + a * p
         r = r - a * Ap
         r0 = r1

@@ -1,0 +1,95 @@
+"""Failure paths of the C ABI on the GPU: every case returns a status and none spins.
+
+The reference only prints when a linear solve or Lanczos stops unconverged
+(FAME_Main/CG.cu:81-84, FAME_Main/Lanczos_Isotropic.cu:84-85) and never checks the
+permittivities it divides by (FAME_Main/FAME_Matrix_B_Isotropic.cu:62-66).  Here:
+  - a NaN, zero or negative permittivity is FAME_ERR_BAD_INPUT;
+  - an A_r^-1 solve that stops above ls_tol sets FAME_KSTATUS_CG on its k-point and
+    the call returns FAME_ERR_NO_CONVERGENCE (FP64: ls_maxit = 1; mixed: one FP32
+    product per inner solve, so the refinement cap is reached);
+  - Lanczos without restarts (es_maxit = 0) at a tight tolerance sets
+    FAME_KSTATUS_LANCZOS;
+  - a loop bound set with fame_set_loop_cap that the CG loop reaches ends the solve
+    with FAME_ERR_WATCHDOG, and the context stays usable afterwards.
+All inputs are host-side; no kernel is made to fault or hang."""
+import numpy as np
+import pytest
+
+import fame_b200 as fb
+from fixtures import edge_eps, load_pre, load_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(name="sc16"):
+    par = load_pre(name)
+    ctx = fb.Context.from_par(par)
+    ctx.set_material(par["binout"], par["material_num"], par["eps_in"], par["eps_out"])
+    return par, ctx
+
+
+@pytest.mark.parametrize("bad", [np.nan, 0.0, -2.0, np.inf])
+def test_bad_permittivity_is_rejected(bad):
+    par, ctx = _ctx()
+    B = edge_eps(par)
+    B[123] = bad
+    with pytest.raises(fb.FameError) as e:
+        ctx.set_eps(B)
+    assert e.value.code == fb.ERR_BAD_INPUT
+    assert "permittivity" in str(e.value)
+    # the context keeps its previous permittivity and still solves
+    k = par["kpoints"][1:2]
+    out = ctx.solve(k, nwant=4, nstep=20, es_tol=1e-8, ls_tol=1e-8)
+    assert out["rc"] == fb.OK
+    ctx.close()
+
+
+@pytest.mark.parametrize("precision", [fb.FP64, fb.MIXED])
+def test_linear_solve_cap_reports_no_convergence(precision):
+    par, ctx = _ctx()
+    k = par["kpoints"][1:3]
+    kw = dict(nwant=4, nstep=20, es_tol=1e-10, es_maxit=1, ls_tol=1e-12, precision=precision)
+    if precision == fb.FP64:
+        kw["ls_maxit"] = 1
+    else:
+        kw["inner_maxit"] = 1
+    out = ctx.solve(k, **kw)
+    assert out["rc"] == fb.ERR_NO_CONVERGENCE
+    for c in out["counters"]:
+        assert c["status"] == fb.ERR_NO_CONVERGENCE
+        assert c["detail"] & fb.KSTATUS_CG
+    assert "ls_tol" in fb.load().fame_last_error().decode()
+    ctx.close()
+
+
+def test_lanczos_without_restarts_reports_no_convergence():
+    par, ctx = _ctx()
+    ref = load_ref("sc16")
+    # the reference restarts at least once on these k-points at 1e-10
+    idx = [i for i, r in enumerate(ref["kpoints"]) if r["es_iter"] > 40][:2]
+    assert idx
+    k = par["kpoints"][idx]
+    out = ctx.solve(k, nwant=10, nstep=40, es_tol=1e-12, es_maxit=0, ls_tol=1e-12)
+    assert out["rc"] == fb.ERR_NO_CONVERGENCE
+    for c in out["counters"]:
+        assert c["detail"] & fb.KSTATUS_LANCZOS
+        assert c["restarts"] == 0
+    ctx.close()
+
+
+@pytest.mark.parametrize("precision", [fb.FP64, fb.MIXED])
+def test_loop_cap_ends_the_solve_with_watchdog(precision):
+    par, ctx = _ctx()
+    k = par["kpoints"][1:2]
+    kw = dict(nwant=4, nstep=20, es_tol=1e-10, ls_tol=1e-10, precision=precision)
+    ctx.set_loop_cap(3)  # the CG needs about 30 products per A_r^-1 at this tolerance
+    with pytest.raises(fb.FameError) as e:
+        ctx.solve(k, **kw)
+    assert e.value.code == fb.ERR_WATCHDOG
+    ctx.set_loop_cap(0)
+    out = ctx.solve(k, **kw)
+    assert out["rc"] == fb.OK
+    assert out["relres"].max() < 1e-6
+    with pytest.raises(fb.FameError):
+        ctx.set_loop_cap(-1)
+    ctx.close()

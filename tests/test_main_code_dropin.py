@@ -72,6 +72,23 @@ def test_dropin_without_device_fails_loudly(tmp_path):
     assert not os.path.exists(os.path.join(d, "Data_Omega_array.txt"))
 
 
+def test_dropin_too_few_permittivities_is_a_status_not_a_prompt(tmp_path):
+    """Four materials and one inner permittivity in Popt.txt: the reference asks for the
+    missing values on stdin (FAME_Main/FAME_Matrix_B_Isotropic.cu:13-24); the drop-in
+    reports the error and returns before any device call, reading nothing from stdin
+    (values offered there are ignored) and writing no frequencies."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("fame_b200_main not built (needs the reference sources)")
+    d = str(tmp_path / "w")
+    build, nx, pn, _, eps_out, nw, ns = ri.WORKLOADS["bcc12"]
+    ri.write_workdir(d, "Syn_bcc12", build(), nx, pn, [10.0], eps_out, nw, ns, 1e-10, 100, 1e-10, 1000)
+    r = subprocess.run([DROPIN], cwd=d, input="9.0\n9.0\n9.0\n9.0\n", capture_output=True, text=True,
+                       timeout=300)
+    assert "1 inner permittivities given for 4 materials" in r.stderr
+    assert "Please input" not in r.stdout
+    assert not os.path.exists(os.path.join(d, "Data_Omega_array.txt"))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["sc16", "fcc16"])
 def test_dropin_matches_reference_main(tmp_path, name):
