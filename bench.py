@@ -154,46 +154,48 @@ def rank_kpoints(W, rank):
     return k
 
 
-def cpu_baseline(W, es_mean, counters):
-    """The oracle (numpy/scipy FP64 restatement of the reference method) timed on the
-    host cores: one A_r^-1 application (full CG to the bench tolerance) at a non-Gamma k of the
-    path, scaled by the mean A_r^-1 count per k-point of this run."""
+def cpu_baseline(W, counters):
+    """The plain FP64 method on the host cores: oracle/fame_cpu.cpp (the C++/OpenMP
+    restatement of the reference's Lanczos / CG / FFT operator, all host threads).
+    Measured end to end on the two small simple-cubic workloads (SC 16^3: two
+    k-points of its path, 10 bands; SC 32^3 with the 96^3 material: k = (0.25, 0, 0),
+    8 bands; tolerance 1e-10).  At 96^3 the time of one CG iteration and of one
+    Lanczos step (j = 25) are measured and scaled by the counters of the FP64 solve
+    (CG iterations, Lanczos steps per k-point): the `value`, labelled extrapolated."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import fame_oracle as fo
-    import scipy.fft as sfft
-    cores = os.cpu_count() or 1
-    par = dict(simple=W["simple"], grid=W["grid"], mesh_len=W["mesh_len"], lattice_vec_a=W["lattice_vec_a"],
-               m=W["m"], t1=W["t1"])
-    N = int(np.prod(W["grid"]))
-    B = fo.matrix_B(W["binout"], W["material_num"], W["eps_in"], W["eps_out"], N)
-    k = W["kpoints"][1]
-    L = fo.lambdas(k, par)
-    rng = np.random.default_rng(0)
-    u = rng.standard_normal(2 * L.Nd) + 1j * rng.standard_normal(2 * L.Nd)
-    u /= np.linalg.norm(u)
-    cnt = {"ls_iter": 0, "es_iter": 0}
-    with sfft.set_workers(cores):
-        # route the oracle's numpy FFT calls through scipy.fft's multithreaded backend
-        saved = (np.fft.fftn, np.fft.ifftn)
-        np.fft.fftn = lambda a, *x, **y: sfft.fftn(a, workers=cores)
-        np.fft.ifftn = lambda a, *x, **y: sfft.ifftn(a, workers=cores)
-        try:
-            t0 = time.perf_counter()
-            fo.invAr(u, L, 1.0 / B, TOLS["ls_tol"], TOLS["ls_maxit"], cnt)
-            t = time.perf_counter() - t0
-        finally:
-            np.fft.fftn, np.fft.ifftn = saved
-    per_k = t * es_mean
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import fame_cpu as fc
+    from fixtures import edge_eps as fx_edge_eps, load_pre
+    cores = fc.threads()
     cpu = ""
     try:
         with open("/proc/cpuinfo") as f:
             cpu = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), "")
     except OSError:
         pass
-    return {"value": 1.0 / per_k, "unit": "k-points/s", "cores": cores, "kind": "port", "cpu_model": cpu,
-            "sample": f"oracle (numpy+scipy.fft FP64) A_r^-1 at 96^3 k={[float(v) for v in np.round(k, 4)]}: "
-                      f"{cnt['ls_iter']} CG products in {t:.2f}s, x mean {es_mean:.1f} A_r^-1 per k "
-                      f"(Lanczos reorthogonalisation not included: lower bound on CPU time)"}
+    measured = {}
+    p16 = load_pre("sc16")
+    o = fc.solve(p16, fx_edge_eps(p16), p16["kpoints"][1:3], 10, 40, 1e-10, 100, 1e-10, 1000)
+    measured["sc16_2k"] = {"kpoints_per_s": round(2 / float(np.sum(o["wall_s"])), 4),
+                           "es_iter": [int(v) for v in o["es_iter"]], "ls_iter": [int(v) for v in o["ls_iter"]]}
+    p32 = load_pre("sc32")
+    o = fc.solve(p32, fx_edge_eps(p32), [[0.25, 0.0, 0.0]], 8, 40, 1e-10, 100, 1e-10, 1000)
+    measured["sc32_1k"] = {"kpoints_per_s": round(1 / float(np.sum(o["wall_s"])), 4),
+                           "es_iter": int(o["es_iter"][0]), "ls_iter": int(o["ls_iter"][0])}
+    N = int(np.prod(W["grid"]))
+    B = edge_eps(W, N)
+    par = dict(grid=W["grid"], mesh_len=W["mesh_len"], lattice_vec_a=W["lattice_vec_a"], simple=True)
+    t_cg, t_lz = fc.time_blocks(par, B, W["kpoints"][1], iters=10, jstep=25)
+    per_k = [c["ls_iter"] * t_cg + c["es_iter"] * t_lz for c in counters]
+    value = len(per_k) / float(np.sum(per_k))
+    return {"value": value, "unit": "k-points/s", "cores": cores, "kind": "port", "cpu_model": cpu,
+            "extrapolated": True, "measured": measured,
+            "sample": f"oracle/fame_cpu.cpp (C++/OpenMP FP64 plain method, {cores} threads): at 96^3 "
+                      f"{t_cg:.4f} s per CG iteration and {t_lz:.4f} s per Lanczos step, times the FP64 solve's "
+                      f"{int(sum(c['ls_iter'] for c in counters))} CG iterations and "
+                      f"{int(sum(c['es_iter'] for c in counters))} Lanczos steps over {len(per_k)} k-points "
+                      "(extrapolated; restart rotations not counted); end-to-end solves of SC16 and SC32 in "
+                      "`measured`"}
 
 
 def solve_bytes(counters, N, nwant, nstep, mixed):
@@ -247,12 +249,28 @@ def run_ours(args):
         kp = kp[: args.nk]
     nk = kp.shape[0]
     prec = fb.MIXED if args.precision == "mixed" else fb.FP64
+    # the FFT plan autotuner (fame_tune) on this grid and batch, before anything is timed
+    plan = ctx.tune(W["kpoints"][1], prec, batch=min(args.batch or nk, 64)) if not args.option else "options"
+    apply_options(ctx, args)
     params = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=prec, batch=args.batch,
                               use_graph=0 if args.no_graph else 1, **TOLS)
     stream = torch.cuda.ExternalStream(ctx.stream())
     out = None
-    for _ in range(args.warmup):
-        out = ctx.solve(kp, params)
+    strong = args.scaling == "strong"
+    costs = None
+    if strong:
+        # strong scaling: the one 20-point path split over the ranks (fame_b200.shard),
+        # blocks balanced by each k-point's CG iterations in the first warm-up solve
+        from fame_b200.shard import solve_sharded
+        kp = W["kpoints"][: args.nk] if args.nk else W["kpoints"]
+        nk = kp.shape[0]
+        run = lambda: solve_sharded(ctx, kp, params, costs=costs)
+    else:
+        run = lambda: ctx.solve(kp, params)
+    for w in range(args.warmup):
+        out = run()
+        if strong and w == 0:
+            costs = [c["ls_iter"] for c in out["counters"]]
     barrier(dist)
     torch.cuda.synchronize()
     l0 = ctx.launch_count()
@@ -261,7 +279,7 @@ def run_ours(args):
     with Clocks(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
-            out = ctx.solve(kp, params)
+            out = run()
         ev1.record(stream)
         ev1.synchronize()
     torch.cuda.synchronize()
@@ -269,7 +287,7 @@ def run_ours(args):
     dt = ev0.elapsed_time(ev1) / 1e3
     launches = ctx.launch_count() - l0
     T = max_over_ranks(dt, dist)
-    value = nk * ws * args.steps / T
+    value = nk * (1 if strong else ws) * args.steps / T
     # ---- end to end through the public API: host eps -> device, solve, host results
     B_host = edge_eps(W, N)
     e2e_steps = max(1, min(args.steps, 2))
@@ -278,10 +296,10 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         ctx.set_eps(B_host)
-        out_e2e = ctx.solve(kp, params)
+        out_e2e = run()
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e = {"value": nk * ws * e2e_steps / t_e2e, "unit": "k-points/s", "h2d_bytes_per_step": int(B_host.nbytes + kp.nbytes),
+    e2e = {"value": nk * (1 if strong else ws) * e2e_steps / t_e2e, "unit": "k-points/s", "h2d_bytes_per_step": int(B_host.nbytes + kp.nbytes),
            "d2h_bytes_per_step": int(3 * nk * NWANT * 8 + nk * 24), "steps": e2e_steps}
     # ---- accuracy of this run
     relres_max = float(np.max(out["relres"]))
@@ -322,10 +340,33 @@ def run_ours(args):
             "stage_ms": [round(x, 5) for x in stages],
             "stage_GBps": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(stage_bytes, stages)],
             "l2": "flushed (256 MiB write) before every launch"}
+    # ---- the dominant work of the mixed solve: one FP32 CG iteration (3 fused kernels)
+    # on a batch of nb k-points; the line's `roofline` is this one, the QBQ apply beside it
+    if prec == fb.MIXED:
+        roof_qbq = roof
+        msc, stc = ctx.bench_cg(kq, reps=10, nbatch=nb)
+        algc = nb * cg_iter_bytes(N)
+        ach = algc / (msc * 1e-3) / 1e9
+        trc = None
+        tp = os.path.join(ROOT, "profiles", "cg_iter_96cubed_traffic.json")
+        if os.path.exists(tp):
+            tj = json.load(open(tp))
+            if tj.get("grid") == list(W["grid"]):
+                trc = int(nb * tj["dram_bytes_per_kpoint"])
+        roof = {"bound": "hbm", "kernel": f"FP32 CG iteration = plane_inv<IN_CG> + pencil<PEN_QBQ_CG> + "
+                                          f"plane_fwd<EPI_CGR> over a batch of {nb} k-points",
+                "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                "peak_source": src, "traffic": trc, "algorithmic_bytes": algc, "batch": nb,
+                "ms_per_launch": round(msc, 5), "us_per_kpoint": round(msc * 1e3 / nb, 2),
+                "stage_ms": [round(x, 5) for x in stc],
+                "stage_GBps": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(
+                    [nb * (10 * N * 8 + 3 * N * 8), nb * (6 * N * 8 + 3 * N * 4), nb * (3 * N * 8 + 4 * N * 8)], stc)],
+                "l2": "flushed (256 MiB write) before every iteration", "qbq_apply": roof_qbq}
     # ---- the plain FP64 form on the same path (the metric's comparison): FP64, one
     # k-point at a time (batch 1) as the reference runs it, every k-point of the path,
     # in the CUDA graph; and FP64 batched like the mixed solve, for comparison
     fp64 = None
+    fp64_counters = None
     if prec == fb.MIXED and not args.no_fp64:
         def timed_solve(p):
             ctx.solve(kp[:1], p)  # records and instantiates the graph of this configuration
@@ -340,6 +381,7 @@ def run_ours(args):
         pb = fb.solver_params(nwant=NWANT, nstep=NSTEP, precision=fb.FP64, batch=args.batch, **TOLS)
         ob, tb = timed_solve(pb)
         nz = o1["freq"] > 0
+        fp64_counters = o1["counters"]
         v1, vb = nk * ws / t1, nk * ws / tb
         fp64 = {"value": v1, "unit": "k-points/s", "batch": 1, "graph": True, "kpoints": nk,
                 "speedup_mixed_over_fp64": round(value / v1, 3),
@@ -361,15 +403,16 @@ def run_ours(args):
         solve_roof = None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(W, es_mean, counters)
+        cpu = cpu_baseline(W, fp64_counters if fp64_counters is not None else counters)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": "k-points/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(T / args.steps * 1e3, 2), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c64 operator/CG + f64 refinement/Lanczos"
+            "scaling": args.scaling, "vs_baseline": None, "dtype": "c64 operator/CG + f64 refinement/Lanczos"
             if prec == fb.MIXED else "f64", "data": "synthetic (reference preprocessing of a synthetic SC crystal)",
             "config": bench_config(nk, ws),
             "run": {"precision": args.precision, "batch": args.batch or "auto", "graph": not args.no_graph,
+                    "fft_plan": plan,
                     "l2": "inputs exceed L2 per step (>1000 CG iterations per step)",
                     "vectors": "eigenvalues only (want_vectors 0); the reference arm's timed region also "
                                "restores E and copies it to the host (about 2% of its time)"},
@@ -385,6 +428,48 @@ def run_ours(args):
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def cg_iter_bytes(N):
+    """Algorithmic bytes of one fused FP32 CG iteration per k-point: read r, p, x and
+    write p, x (7M.8 with the r read and write of the residual update), the field out
+    of the inverse plane stage, through the pencil stage and into the forward plane
+    stage (12N.8), and 1/eps (3N.4)."""
+    M = 2 * N
+    return 7 * M * 8 + 12 * N * 8 + 3 * N * 4
+
+
+def apply_options(ctx, args):
+    """--option name=value: execution options of the context (fame_set_option)."""
+    for o in args.option:
+        n, v = o.split("=")
+        ctx.set_option(n, int(v))
+
+
+def run_cg(args):
+    """FP32 CG iterations alone (fame_bench_cg, 96^3 or --workload; one k off Gamma
+    repeated --batch times), each preceded by a 256 MiB L2 flush: the small case of the
+    CG-kernel profiles in profiles/."""
+    import fame_b200 as fb
+    if args.workload == WORKLOAD:
+        W = load_workload()
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from fixtures import load_pre
+        W = load_pre(args.workload)
+    ctx = fb.Context(W["grid"], W["mesh_len"], W["lattice_vec_a"], W["simple"], W["m"], W["t1"])
+    ctx.set_material(W["binout"], W["material_num"], W["eps_in"], W["eps_out"])
+    apply_options(ctx, args)
+    nb = max(1, args.batch)
+    ms, st = ctx.bench_cg(W["kpoints"][1], reps=max(1, args.steps), nbatch=nb)
+    N = int(np.prod(W["grid"]))
+    hbm, src = peaks()
+    gbs = nb * cg_iter_bytes(N) / (ms * 1e-3) / 1e9
+    print(json.dumps({"mode": "cg", "workload": args.workload, "grid": list(W["grid"]), "reps": args.steps,
+                      "batch": nb, "ms_per_iteration": round(ms, 5), "us_per_kpoint": round(ms * 1e3 / nb, 2),
+                      "stage_ms": [round(x, 5) for x in st], "GBps": round(gbs, 1),
+                      "frac_of_measured_hbm": round(gbs / hbm, 4), "options": args.option}), flush=True)
+    ctx.close()
 
 
 def run_qbq(args):
@@ -436,6 +521,14 @@ def run_lattices(args):
                 "tol": ref["tol"],
                 "reference_kps": round(len(ref["kpoints"]) / sum(r["wall_s"] for r in ref["kpoints"]), 3)}
         rk = {tuple(np.round(r["wave_vec"], 12)): np.array(r["freq"]) for r in ref["kpoints"]}
+        # operator times per k-point (batch 8): the built-in plan, then the tuned one
+        kq = k[0]
+        line["cg_us_per_kpoint_default_plan"] = round(ctx.bench_cg(kq, reps=5, nbatch=8)[0] * 1e3 / 8, 2)
+        line["qbq64_us_per_kpoint_default_plan"] = round(ctx.bench_qbq(kq, fb.FP64, reps=5, nbatch=8)[0] * 1e3 / 8, 2)
+        line["fft_plan_fp64"] = ctx.tune(kq, fb.FP64, batch=8)
+        line["qbq64_us_per_kpoint_tuned"] = round(ctx.bench_qbq(kq, fb.FP64, reps=5, nbatch=8)[0] * 1e3 / 8, 2)
+        line["fft_plan_mixed"] = ctx.tune(kq, fb.MIXED, batch=8)
+        line["cg_us_per_kpoint_tuned"] = round(ctx.bench_cg(kq, reps=5, nbatch=8)[0] * 1e3 / 8, 2)
         for prec, tag in ((fb.MIXED, "mixed"), (fb.FP64, "fp64")):
             p = fb.solver_params(nwant=nw, nstep=NSTEP, es_tol=ref["tol"], ls_tol=ref["tol"], es_maxit=100,
                                  ls_maxit=1000, precision=prec)
@@ -560,7 +653,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "qbq", "locate", "lattices"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "qbq", "cg", "locate", "lattices"],
                     help="qbq: only time Q_r^* B^-1 Q_r applies (--steps applies; for kernel profiles); "
                          "lattices: band solves of the FCC, BCC and hexagonal workloads")
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD] + [n for n, _ in LATTICES],
@@ -569,12 +662,18 @@ def main():
                     help="host-driven loops instead of the CUDA graph (launch lists under ncu)")
     ap.add_argument("--nk", type=int, default=0, help="solve only the first NK k-points (launch-list samples)")
     ap.add_argument("--tol", type=float, default=TOLS["es_tol"], help="Lanczos and CG tolerance")
+    ap.add_argument("--option", action="append", default=[], help="execution option name=value (fame_set_option)")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="weak: every rank solves its own 20-point path; strong: the ranks split one path "
+                         "(cost-balanced blocks, one gather)")
     args = ap.parse_args()
     TOLS["es_tol"] = TOLS["ls_tol"] = args.tol
     if args.impl == "reference":
         return run_reference(args)
     if args.mode == "qbq":
         return run_qbq(args)
+    if args.mode == "cg":
+        return run_cg(args)
     if args.mode == "locate":
         return run_locate(args)
     if args.mode == "lattices":

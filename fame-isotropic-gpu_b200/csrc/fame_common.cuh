@@ -113,6 +113,17 @@ template <int N> __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Bulk prefetch into L2 (cp.async.bulk.prefetch.L2, sm_90+) of the 16-byte-aligned
+// part of [p, p + bytes): the start is rounded up and the end down to 16 bytes, so
+// nothing outside the range is touched.  A hint only: no data reaches the thread.
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+  const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
+  if (e <= a) return;
+  const unsigned n = (unsigned)(e - a);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"(n) : "memory");
+}
+
 // Kernels launched on the device, counted by each kernel's first thread.  Every
 // translation unit has its own counter; FAME_DEFINE_LAUNCH_GETTER exposes it.
 static __device__ unsigned long long g_launches;

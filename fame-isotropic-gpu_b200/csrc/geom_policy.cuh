@@ -78,6 +78,17 @@ struct StatGeom {
     constexpr int TW = PencilTW<R>::v;
     sfft<R, LSL, TW, kPencilThreads, SPenEmax<R>::v>(b, 1, TW, tw, inv);
   }
+  // The same passes with the axis and the direction fixed at compile time: every
+  // stride, twiddle sign and rotation folds to a constant (one call site each).
+  template <typename R, bool FAST, bool INV>
+  __device__ __forceinline__ static void fft_plane_c(cplx<R>* b, const cplx<R>* tw) {
+    sfft<R, LF, LM, kStatPlaneThreads, SEmax<R>::v>(b, FAST ? kS : 1, FAST ? 1 : kS, tw, INV);
+  }
+  template <typename R, bool INV>
+  __device__ __forceinline__ static void fft_slow_c(cplx<R>* b, const cplx<R>* tw) {
+    constexpr int TW = PencilTW<R>::v;
+    sfft<R, LSL, TW, kPencilThreads, SPenEmax<R>::v>(b, 1, TW, tw, INV);
+  }
 };
 
 using Stat96 = StatGeom<96, 96, 96>;

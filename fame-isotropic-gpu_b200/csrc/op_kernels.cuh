@@ -27,6 +27,37 @@ __device__ __forceinline__ void lam_elem(const Geom& g, const double2* tab, cons
   }
 }
 
+// ------------------------------------------------------------------ L2 prefetch
+// The CTAs of a stage kernel run in waves in launch order, and each one spends most of
+// its time on shared-memory transforms.  A CTA therefore issues, at its start, bulk L2
+// prefetches of the global operands of the CTA pf_dist places later (about one wave
+// ahead), so that CTA finds them in L2 instead of waiting on DRAM.  The prefetches only
+// cover bytes that CTA will read.
+
+// Linear launch index of this CTA, and the (x, y, z) block of linear index t.
+__device__ __forceinline__ long cta_linear() {
+  return blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
+}
+__device__ __forceinline__ bool cta_of(long t, int& x, int& y, int& z) {
+  const long n = (long)gridDim.x * gridDim.y * gridDim.z;
+  if (t >= n) return false;
+  x = (int)(t % gridDim.x);
+  const long r = t / gridDim.x;
+  y = (int)(r % gridDim.y);
+  z = (int)(r / gridDim.y);
+  return true;
+}
+
+// The reduced-vector range [e0, e1) of plane s that the component-`comp` CTA of a
+// plane cluster mixes, as element offsets (first half; the second starts Nd later).
+__device__ __forceinline__ bool plane_vec_range(int P, int s, int comp, const Slot& sl, long& i0, long& i1) {
+  const int per = (P + 2) / 3;
+  const int e0 = comp * per, e1 = min(P, e0 + per);
+  i0 = max(0L, (long)s * P + e0 - sl.off);
+  i1 = (long)s * P + e1 - sl.off;
+  return i1 > i0;
+}
+
 // One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
 template <typename R, bool GEN, int IN, bool PR, int RARE, class GP>
 __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::kStatic ? (sizeof(R) == 4 ? 2 : 1) : (RARE >= 2 ? 1 : 2))
@@ -55,6 +86,22 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       if (!st->active) return;
     } else {
       if (!st->outer_active) return;
+    }
+  }
+  if constexpr (IN == IN_CG) {
+    // r, p and x of the CTA one wave ahead (p and x once its k-point is past k = 1)
+    int x2, y2, z2;
+    if (a.pf_dist > 0 && threadIdx.x < 6 && cta_of(cta_linear() + a.pf_dist, x2, y2, z2)) {
+      const Slot s2 = a.slots[z2];
+      const CgState* c2 = a.cg + z2;
+      long i0, i1;
+      const int which = threadIdx.x >> 1;  // 0 r, 1 p, 2 x
+      if (s2.active && c2->active && (which == 0 || c2->iter > 1) &&
+          plane_vec_range(P, x2 / 3, x2 % 3, s2, i0, i1)) {
+        const cplx<R>* v = which == 0 ? a.r : which == 1 ? a.p : a.x;
+        const long base = (long)(z2 * a.vec_per_slot + y2) * a.vstride + ((threadIdx.x & 1) ? s2.Nd : 0);
+        prefetch_l2(v + base + i0, (i1 - i0) * sizeof(cplx<R>));
+      }
     }
   }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
@@ -101,7 +148,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   // inner solve's last update folded in.  The operands of KB points per thread are
   // loaded up front, so one global-load latency covers KB points.
   // (runtime geometries run at 64 registers: two points)
-  constexpr int KB = !GP::kStatic ? 2 : IN == IN_VEC ? 8 : (sizeof(R) == 4 ? 4 : 2);
+  constexpr int KB = !GP::kStatic ? 2 : IN == IN_VEC ? 8 : 2;
   const int NT = GP::plane_threads();
   for (int eb = e0 + threadIdx.x; eb < e1; eb += KB * NT) {
     cplx<R> A1[KB], A2[KB], B1[KB], B2[KB], C1[KB], C2[KB];
@@ -198,7 +245,11 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   // inverse 2-D transform of this component's plane (unnormalised): fast axis,
   // then mid axis.  One FFT call site per axis loop keeps the kernel within its
   // register budget.
-  for (int ax = 0; ax < 2; ax++) {
+  if constexpr (GP::kStatic && !GEN) {
+    GP::template fft_plane_c<R, true, true>(plane, twf);
+    GP::template fft_plane_c<R, false, true>(plane, twm);
+  }
+  for (int ax = 0; !(GP::kStatic && !GEN) && ax < 2; ax++) {
     GP::template fft_plane<R, RARE>(plane, g, ax == 0, ax == 0 ? twf : twm, true);
     if constexpr (GEN) {
       // x D_kz(x,y,z) after the z (fast) pass (FAME_FFT_CUDA.cu:109, kernel :283-317),
@@ -244,6 +295,21 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
   const int m = blockIdx.x / nft;
   const int f0 = (blockIdx.x - m * nft) * TW;
   const int tw_n = min(TW, Lf - f0);
+  if constexpr (MODE == PEN_QBQ_CG) {
+    // the field rows and 1/eps rows of the tile of the CTA one wave ahead
+    int x2, y2, z2;
+    if (a.pf_dist > 0 && threadIdx.x < 2 * Ls && cta_of(cta_linear() + a.pf_dist, x2, y2, z2) &&
+        a.slots[z2].active && a.cg[z2].active) {
+      const int m2 = x2 / nft, f2 = (x2 - m2 * nft) * TW, c2 = y2 % 3, v2 = y2 / 3;
+      const int n2 = min(TW, Lf - f2);
+      const int srow = threadIdx.x < Ls ? threadIdx.x : threadIdx.x - Ls;
+      const long off = (long)c2 * g.N + (long)srow * P + m2 * Lf + f2;
+      if (threadIdx.x < Ls)
+        prefetch_l2(a.T + (long)(z2 * a.vec_per_slot + v2) * a.fstride + off, n2 * sizeof(cplx<R>));
+      else
+        prefetch_l2(a.invB + off, n2 * sizeof(R));
+    }
+  }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
   for (int i = threadIdx.x; i < Ls; i += kPencilThreads) tws[i] = a.tw[g.tws + i];
   const long fb = (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N;
@@ -295,7 +361,21 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
   constexpr int ndir = QBQ ? 2 : 1;
   // PEN_QBQ_CG: sum of |v|^2 / eps over the tile after the inverse transform
   float dot = 0.f;
-  for (int dir = 0; dir < ndir; dir++) {
+  constexpr bool kStatQBQ = GP::kStatic && QBQ;  // whole tiles, 1/eps staged in shared memory
+  if constexpr (kStatQBQ) {
+    GP::template fft_slow_c<R, true>(tile, tws);
+    const R invN = (R)(1.0 / g.N);
+#pragma unroll 4
+    for (int q = threadIdx.x; q < Ls * TW; q += kPencilThreads) {
+      const R ib = ibt[q];
+      const cplx<R> v = tile[q];
+      if constexpr (MODE == PEN_QBQ_CG) dot += (float)(ib * cabs2(v));
+      tile[q] = cscale(v, ib * invN);
+    }
+    __syncthreads();
+    GP::template fft_slow_c<R, false>(tile, tws);
+  }
+  for (int dir = 0; !kStatQBQ && dir < ndir; dir++) {
     const bool inv = MODE == PEN_QRS_IN ? false : dir == 0;
     GP::template fft_slow<R, RARE>(tile, g, tws, inv);
     if (MODE != PEN_QRS_IN && dir == 0) {
@@ -418,8 +498,7 @@ __global__ void __launch_bounds__(kPencilThreads, sizeof(R) == 4 ? 3 : 2) k_penc
   constexpr int Lf = 96, Lm = 96, Ls = 96, P = Lf * Lm;
   constexpr int nft = Lf / TW;
   constexpr int TILE = Ls * TW;
-  constexpr int CH = 16 / sizeof(cplx<R>);  // elements per 16-byte copy
-  constexpr int CHB = 16 / sizeof(R);       // 1/eps values per 16-byte copy
+  constexpr int CHB = 16 / sizeof(R);  // 1/eps values per 16-byte copy
   static_assert(Lf % TW == 0 && TW % CHB == 0, "whole tiles of whole 16-byte copies");
   cplx<R>* tiles = reinterpret_cast<cplx<R>*>(smem_raw);     // [2][TILE]
   R* ibts = reinterpret_cast<R*>(tiles + 2 * TILE);            // [2][TILE]
@@ -502,6 +581,27 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     if constexpr (EPI == EPI_RESID || EPI == EPI_CGR) plane_fwd_decide<EPI>(a);
     return;
   }
+  if constexpr (EPI == EPI_CGR) {
+    // the field plane (4 pieces) and the residual of the CTA one wave ahead
+    int x2, y2, z2;
+    if (a.pf_dist > 0 && threadIdx.x < 6 && cta_of(cta_linear() + a.pf_dist, x2, y2, z2)) {
+      const Slot s2 = a.slots[z2];
+      if (s2.active && a.cg[z2].active) {
+        const int s2p = x2 / 3, c2 = x2 % 3;
+        if (threadIdx.x < 4) {
+          const long piece = (P + 3) / 4;
+          const long lo = threadIdx.x * piece, hi = min((long)P, lo + piece);
+          prefetch_l2(a.T + (long)(z2 * a.vec_per_slot + y2) * a.fstride + (long)c2 * g.N + (long)s2p * P + lo,
+                      (hi - lo) * sizeof(cplx<R>));
+        } else {
+          long i0, i1;
+          if (plane_vec_range(P, s2p, c2, s2, i0, i1))
+            prefetch_l2(a.r + (long)(z2 * a.vec_per_slot + y2) * a.vstride + ((threadIdx.x & 1) ? s2.Nd : 0) + i0,
+                        (i1 - i0) * sizeof(cplx<R>));
+        }
+      }
+    }
+  }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
   for (int i = threadIdx.x; i < Lf; i += GP::plane_threads()) {
     twf[i] = a.tw[g.twf + i];
@@ -522,7 +622,11 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   // forward 2-D transform.  General lattices (T*, FAME_FFT_CUDA.cu:128-150):
   // x conj(D_ky), y (mid) pass, x conj(D_kz), z (fast) pass.  Simple lattices:
   // fast then mid axis, no twiddles.
-  for (int ax = 0; ax < 2; ax++) {
+  if constexpr (GP::kStatic && !GEN) {
+    GP::template fft_plane_c<R, true, false>(plane, twf);
+    GP::template fft_plane_c<R, false, false>(plane, twm);
+  }
+  for (int ax = 0; !(GP::kStatic && !GEN) && ax < 2; ax++) {
     const bool fast = GEN ? ax == 1 : ax == 0;
     if constexpr (GEN) {
       for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {

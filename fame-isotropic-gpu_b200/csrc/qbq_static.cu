@@ -39,6 +39,7 @@
 #include <string>
 
 #include "../../include/fame_b200.h"
+#include "geometry.h"
 #include "op_kernels_decl.h"
 
 namespace fame {
@@ -73,110 +74,6 @@ __global__ void k_static_prep(Slot sl, Geom g, Slot* slot, double2* tw) {
       sincospi(2.0 * i / n[a], &s, &c);
       tw[o[a] + i] = make_double2(c, -s);
     }
-}
-
-bool factor_axis(int n, AxisPlan& p) {
-  // radix order of the solver's plans: 8, 4, 2, 5, 3, 7, 11, 13, then larger primes
-  p.n = n;
-  p.npass = 0;
-  int m = n;
-  const int order[] = {8, 4, 2, 5, 3, 7, 11, 13};
-  for (int r : order)
-    while (m % r == 0) {
-      if (p.npass >= kMaxPasses) return false;
-      p.radix[p.npass++] = r;
-      m /= r;
-    }
-  for (int q = 17; m > 1 && q <= m; q++)
-    while (m % q == 0) {
-      if (p.npass >= kMaxPasses) return false;
-      p.radix[p.npass++] = q;
-      m /= q;
-    }
-  return m == 1;
-}
-
-// Geometry of the lattice (the layout the solver's context sets up).
-int make_geom(const fame_lattice& L, Geom& g, int& rare, int& threads) {
-  memset(&g, 0, sizeof(g));
-  g.Nx = L.grid[0];
-  g.Ny = L.grid[1];
-  g.Nz = L.grid[2];
-  if (g.Nx < 2 || g.Ny < 2 || g.Nz < 2) {
-    set_last_error("grid dimensions must be >= 2");
-    return FAME_ERR_BAD_INPUT;
-  }
-  const long N = (long)g.Nx * g.Ny * g.Nz;
-  if (N > (1L << 24)) {
-    set_last_error("grid too large");
-    return FAME_ERR_UNSUPPORTED;
-  }
-  g.N = (int)N;
-  g.general = L.simple ? 0 : 1;
-  g.hx = L.mesh_len[0];
-  g.hy = L.mesh_len[1];
-  g.hz = L.mesh_len[2];
-  g.Ls = g.general ? g.Nx : g.Nz;
-  g.Lm = g.Ny;
-  g.Lf = g.general ? g.Nz : g.Nx;
-  g.P = g.Lm * g.Lf;
-  g.S = g.Lf | 1;
-  if (!factor_axis(g.Lf, g.pf) || !factor_axis(g.Lm, g.pm) || !factor_axis(g.Ls, g.ps)) {
-    set_last_error("axis length needs more than 10 FFT passes");
-    return FAME_ERR_UNSUPPORTED;
-  }
-  rare = std::max(plan_level(g.pf), std::max(plan_level(g.pm), plan_level(g.ps)));
-  threads = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
-  if (plane_smem_bytes<double>(g.Lf, g.Lm, g.S) > 227 * 1024) {
-    set_last_error("plane exceeds one CTA");
-    return FAME_ERR_UNSUPPORTED;
-  }
-  int o = 0;
-  if (!g.general) {
-    g.oLx = o; o += g.Nx;
-    g.oLy = o; o += g.Ny;
-    g.oLz = o; o += g.Nz;
-    g.oDx = o; o += g.Nx;
-    g.oDy = o; o += g.Ny;
-    g.oDz = o; o += g.Nz;
-  } else {
-    g.oLx = o; o += g.Nx;
-    g.oLy = o; o += g.Nx * g.Ny;
-    g.oExy = o; o += g.Nx * g.Ny;
-    g.oWz = o; o += g.Nz;
-    g.oDky = o; o += g.Nx * g.Ny;
-    g.oPhi = o; o += g.Nx * g.Ny;
-    g.oDkx = o; o += g.Nx;
-  }
-  g.tab_stride = (o + 7) / 8 * 8;
-  g.twf = 0;
-  g.twm = g.Lf;
-  g.tws = g.Lf + g.Lm;
-  return FAME_OK;
-}
-
-// theta_x, theta_y(xy), theta_z(xyz) of a k-point (FAME_Main/FAME_Matrix_Lambdas.cu:43-70)
-void make_thetas(const fame_lattice& L, const double* k, double th[3]) {
-  const double* a = L.lattice_vec_a;
-  auto dot = [&](const double* v) { return k[0] * v[0] + k[1] * v[1] + k[2] * v[2]; };
-  th[0] = dot(a);
-  if (L.simple) {
-    th[1] = dot(a + 3);
-    th[2] = dot(a + 6);
-    return;
-  }
-  double c1 = 0.0;
-  if (a[3] > 0)
-    c1 = -(double)L.m[0] / (double)L.grid[0];
-  else if (a[3] < 0)
-    c1 = 1. - (double)L.m[0] / (double)L.grid[0];
-  const double c2 = (double)L.m[2] / (double)L.grid[1];
-  const double c3 = (double)L.m[1] / (double)L.grid[0];
-  double a2h[3], a3h[3];
-  for (int i = 0; i < 3; i++) a2h[i] = c1 * a[i] + a[3 + i];
-  for (int i = 0; i < 3; i++) a3h[i] = a[6 + i] - c2 * a2h[i] - c3 * a[i] + L.t1[i];
-  th[1] = dot(a2h);
-  th[2] = dot(a3h);
 }
 
 template <typename K> cudaError_t raise_smem(K* k, size_t bytes) {
@@ -260,10 +157,14 @@ int fame_qbq_static(const fame_lattice* lat, const double* k, const double* inv_
     return FAME_ERR_BAD_INPUT;
   }
   Geom g;
-  int rare = 0;
-  int threads = 0;
-  int rc = make_geom(*lat, g, rare, threads);
-  if (rc != FAME_OK) return rc;
+  std::string err;
+  const int rc = layout_geom(*lat, g, 1L << 24, err);
+  if (rc != FAME_OK) {
+    set_last_error(err);
+    return rc;
+  }
+  const int rare = geom_level(g);
+  const int threads = plane_threads_rule<double>(g, rare);
   const size_t off_tw = align256(sizeof(Slot));
   const size_t off_tab = off_tw + align256(sizeof(double2) * (size_t)(g.Lf + g.Lm + g.Ls));
   const size_t off_T = off_tab + align256(sizeof(double2) * (size_t)g.tab_stride);
@@ -293,14 +194,7 @@ int fame_qbq_static(const fame_lattice* lat, const double* k, const double* inv_
     }
     base = (unsigned char*)g_scratch_ptr[dev];
   }
-  Slot sl;
-  memset(&sl, 0, sizeof(sl));
-  make_thetas(*lat, k, sl.th);
-  const double nrm = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
-  // Gamma point: Nd = N - 1 (FAME_Main/FAME_Matrix_Lambdas.cu:157 Simple, :406 General)
-  sl.Nd = nrm < (lat->simple ? 1e-4 : 1e-3) ? g.N - 1 : g.N;
-  sl.off = g.N - sl.Nd;
-  sl.active = 1;
+  const Slot sl = make_slot(*lat, k);
   Slot* slot = (Slot*)base;
   double2* tw = (double2*)(base + off_tw);
   double2* tabs = (double2*)(base + off_tab);

@@ -21,6 +21,7 @@
 #include <utility>
 
 #include "../../include/fame_b200.h"
+#include "geometry.h"
 #include "op_kernels_decl.h"
 #include "program.h"
 #include "solver_kernels.cuh"
@@ -48,32 +49,6 @@ static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
 // error text of the entry points defined in other translation units
 void set_last_error(const std::string& s) { g_err = s; }
-
-// ------------------------------------------------------------------ FFT plans
-static bool factorize(int n, AxisPlan& p) {
-  p.n = n;
-  p.npass = 0;
-  int m = n;
-  const int order[] = {8, 4, 2, 5, 3, 7, 11, 13};
-  for (int r : order) {
-    while (m % r == 0) {
-      if (p.npass >= kMaxPasses) return false;
-      p.radix[p.npass++] = r;
-      m /= r;
-    }
-  }
-  for (int q = 17; m > 1 && q <= m; q++) {
-    while (m % q == 0) {
-      if (p.npass >= kMaxPasses) return false;
-      p.radix[p.npass++] = q;
-      m /= q;
-    }
-  }
-  if (n == 1) {
-    p.npass = 0;
-  }
-  return m == 1;
-}
 
 // ------------------------------------------------------------------ device buffers
 template <typename T> struct DBuf {
@@ -107,6 +82,10 @@ struct fame_ctx {
   int plane_threads32 = 512;  // the same for FP32 kernels
   template <typename R> int plane_nt() const { return sizeof(R) == 4 ? plane_threads32 : plane_threads; }
   int pipe_ctas64 = 0;  // resident k_pencil_pipe<double> CTAs on the device
+  int prefetch = 0;     // L2 prefetch one wave ahead in the CG stage kernels (fame_set_option; measured slower)
+  int radix_order = 0;  // kRadixOrders index of the runtime-geometry axis plans
+  int threads32_opt = 0, threads64_opt = 0;  // plane CTA sizes set by fame_set_option (0: rule)
+  std::map<const void*, int> waves;  // resident CTAs of a stage kernel on the device
   int rare = 0;         // fft_lines level the axis plans need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   int loop_cap = 0;     // fame_set_loop_cap: bound on every device loop's trips (0: defaults)
@@ -135,6 +114,12 @@ struct fame_ctx {
   DBuf<double2> U, r64, x64, b64, p64, Ap64, T64, EV, AV, Tb, E;
   DBuf<float2> r32, x32, p32, T32;
   int* hflag = nullptr;  // pinned
+  // eigenvectors kept on the device by the last solve (evec_out NULL): its k-points,
+  // whether each is the Gamma point (Gamma keeps nwant - 2 restored bands), nwant
+  int dev_vec_nk = 0, dev_vec_nwant = 0;
+  std::vector<int> dev_vec_gamma;
+  DBuf<double> adj;  // fame_adjoint_vjp: [nwant] w, [nwant] grad_w, [nwant] denominators
+  DBuf<int> eps_bad;  // fame_set_eps_device: [0] bad count, [1] first bad edge
   // recorded programs keyed by configuration
   std::map<std::string, std::unique_ptr<Program>> progs;
 };
@@ -154,6 +139,32 @@ template <typename R> static size_t pencil_smem(const Geom& g) { return pencil_s
 
 template <typename K> static void allow_smem(K* k, size_t bytes) {
   if (bytes > 48 * 1024) FAME_CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// CTAs of a stage kernel resident on the whole device at once (one wave): clusters of
+// three CTAs for the plane kernels (cluster = 3), single CTAs for the pencil kernels.
+// Cached per kernel in the context; 0 if the occupancy query fails.
+template <typename K> static int wave_ctas(fame_ctx* c, K* k, int threads, size_t smem, int cluster) {
+  auto it = c->waves.find((const void*)k);
+  if (it != c->waves.end()) return it->second;
+  int n = 0, dev = 0, sms = 0;
+  if (cluster > 1) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster * 64, 1, 1);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)k, &cfg) == cudaSuccess) n = ncl * cluster;
+  } else {
+    int per = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ==
+                                                   cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, threads, smem) == cudaSuccess)
+      n = per * sms;
+  }
+  cudaGetLastError();  // a failed query only disables the prefetch
+  c->waves[(const void*)k] = n;
+  return n;
 }
 
 // CTAs of kernel k (kPencilThreads threads, `smem` dynamic shared bytes) resident on
@@ -222,6 +233,7 @@ struct Ops {
                : c->rare == 1 ? k_plane_inv<R, true, IN, PR, 1, DynGeom>
                               : k_plane_inv<R, true, IN, PR, 0, DynGeom>;
       allow_smem(k, sm);
+      a.pf_dist = IN == IN_CG && c->prefetch ? wave_ctas(c, k, c->template plane_nt<R>(), sm, 3) : 0;
       P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_inv<R, false, IN, PR, 2, DynGeom>
@@ -234,6 +246,7 @@ struct Ops {
           nt = kStatPlaneThreads;
         }
       allow_smem(k, sm);
+      a.pf_dist = IN == IN_CG && c->prefetch ? wave_ctas(c, k, nt, sm, 3) : 0;
       P.launch(k, grid, dim3(nt), sm, a);
     }
   }
@@ -262,11 +275,13 @@ struct Ops {
     const size_t sm = pencil_smem<R>(g());
     const int nft = (g().Lf + a.TW - 1) / a.TW;
     dim3 grid(g().Lm * nft, 3 * nvec, nslots);
+    a.pf_dist = 0;
     if (g().general) {
       auto k = c->rare == 2   ? k_pencil<R, true, MODE, 2, DynGeom>
                : c->rare == 1 ? k_pencil<R, true, MODE, 1, DynGeom>
                               : k_pencil<R, true, MODE, 0, DynGeom>;
       allow_smem(k, sm);
+      if (MODE == PEN_QBQ_CG && c->prefetch) a.pf_dist = wave_ctas(c, k, kPencilThreads, sm, 1);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
     } else {
       auto k = c->rare == 2   ? k_pencil<R, false, MODE, 2, DynGeom>
@@ -286,6 +301,7 @@ struct Ops {
           return;
         }
       allow_smem(k, sm);
+      if (MODE == PEN_QBQ_CG && c->prefetch) a.pf_dist = wave_ctas(c, k, kPencilThreads, sm, 1);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
     }
   }
@@ -320,6 +336,7 @@ struct Ops {
                : c->rare == 1 ? k_plane_fwd<R, true, EPI, PR, 1, DynGeom>
                               : k_plane_fwd<R, true, EPI, PR, 0, DynGeom>;
       allow_smem(k, sm);
+      a.pf_dist = EPI == EPI_CGR && c->prefetch ? wave_ctas(c, k, c->template plane_nt<R>(), sm, 3) : 0;
       P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_fwd<R, false, EPI, PR, 2, DynGeom>
@@ -332,6 +349,7 @@ struct Ops {
           nt = kStatPlaneThreads;
         }
       allow_smem(k, sm);
+      a.pf_dist = EPI == EPI_CGR && c->prefetch ? wave_ctas(c, k, nt, sm, 3) : 0;
       P.launch(k, grid, dim3(nt), sm, a);
     }
   }
@@ -341,86 +359,22 @@ template <> const float2* Ops::tw<float>() const { return c->tw32.p; }
 
 // ------------------------------------------------------------------ geometry
 static int setup_geom(fame_ctx* c) {
-  const fame_lattice& L = c->lat;
   Geom& g = c->g;
-  memset(&g, 0, sizeof(g));
-  g.Nx = L.grid[0];
-  g.Ny = L.grid[1];
-  g.Nz = L.grid[2];
-  if (g.Nx < 2 || g.Ny < 2 || g.Nz < 2) {
-    set_err("grid dimensions must be >= 2");
-    return FAME_ERR_BAD_INPUT;
+  std::string err;
+  const int rc = layout_geom(c->lat, g, 1L << 28, err);
+  if (rc != FAME_OK) {
+    set_err(err);
+    return rc;
   }
-  const long N = (long)g.Nx * g.Ny * g.Nz;
-  if (N > (1L << 28)) {
-    set_err("grid too large");
-    return FAME_ERR_BAD_INPUT;
-  }
-  g.N = (int)N;
-  g.general = L.simple ? 0 : 1;
-  g.hx = L.mesh_len[0];
-  g.hy = L.mesh_len[1];
-  g.hz = L.mesh_len[2];
-  if (!g.general) {
-    g.Ls = g.Nz;
-    g.Lm = g.Ny;
-    g.Lf = g.Nx;
-  } else {
-    g.Ls = g.Nx;
-    g.Lm = g.Ny;
-    g.Lf = g.Nz;
-  }
-  g.P = g.Lm * g.Lf;
-  g.S = g.Lf | 1;
-  if (!factorize(g.Lf, g.pf) || !factorize(g.Lm, g.pm) || !factorize(g.Ls, g.ps)) {
-    set_err("axis length needs more than 10 FFT passes");
-    return FAME_ERR_UNSUPPORTED;
-  }
-  c->rare = std::max(plan_level(g.pf), std::max(plan_level(g.pm), plan_level(g.ps)));
-  // the whole plane must fit one CTA's shared memory (FP64 copy)
-  // threads of a runtime-geometry plane CTA: about 8 plane elements per thread, at
-  // most 256 when two planes fit in shared memory (more, smaller CTAs per SM hide
-  // the latency of the staged passes better), except FP64 planes with the prime
-  // pass, whose 128-register budget admits one CTA per SM
-  const int pt = std::min(512, std::max(64, ((g.P + 7) / 8 + 31) / 32 * 32));
-  const int kSmemSM = 227 * 1024;
-  c->plane_threads32 = 2 * plane_smem<float>(g) <= (size_t)kSmemSM ? std::min(pt, 256) : pt;
-  c->plane_threads = c->rare < 2 && 2 * plane_smem<double>(g) <= (size_t)kSmemSM ? std::min(pt, 256) : pt;
+  c->rare = geom_level(g);
+  c->plane_threads32 = plane_threads_rule<float>(g, c->rare);
+  c->plane_threads = plane_threads_rule<double>(g, c->rare);
   c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96;
   if (c->stat96) c->pipe_ctas64 = resident_ctas(k_pencil_pipe<double>, pencil_pipe_smem_bytes<double>(g.Ls));
-  if (plane_smem<double>(g) > 227 * 1024) {
-    set_err("plane " + std::to_string(g.Lm) + "x" + std::to_string(g.Lf) + " exceeds one CTA");
-    return FAME_ERR_UNSUPPORTED;
-  }
-  // table offsets
-  int o = 0;
-  if (!g.general) {
-    g.oLx = o; o += g.Nx;
-    g.oLy = o; o += g.Ny;
-    g.oLz = o; o += g.Nz;
-    g.oDx = o; o += g.Nx;
-    g.oDy = o; o += g.Ny;
-    g.oDz = o; o += g.Nz;
-  } else {
-    g.oLx = o; o += g.Nx;
-    g.oLy = o; o += g.Nx * g.Ny;
-    g.oExy = o; o += g.Nx * g.Ny;
-    g.oWz = o; o += g.Nz;
-    g.oDky = o; o += g.Nx * g.Ny;
-    g.oPhi = o; o += g.Nx * g.Ny;
-    g.oDkx = o; o += g.Nx;
-  }
-  g.tab_stride = (o + 7) / 8 * 8;
   // twiddles e^{-2 pi i m / n} for the fast, mid and slow axes
   std::vector<double2> tw;
-  auto add = [&](int n) {
-    const int off = (int)tw.size();
+  for (int n : {g.Lf, g.Lm, g.Ls})  // at g.twf, g.twm, g.tws
     for (int m = 0; m < n; m++) tw.push_back(make_double2(cos(2.0 * M_PI * m / n), -sin(2.0 * M_PI * m / n)));
-    return off;
-  };
-  g.twf = add(g.Lf);
-  g.twm = add(g.Lm);
-  g.tws = add(g.Ls);
   std::vector<float2> tw32(tw.size());
   for (size_t i = 0; i < tw.size(); i++) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
   c->tw64.ensure(tw.size());
@@ -428,37 +382,6 @@ static int setup_geom(fame_ctx* c) {
   FAME_CK(cudaMemcpy(c->tw64.p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
   FAME_CK(cudaMemcpy(c->tw32.p, tw32.data(), tw32.size() * sizeof(float2), cudaMemcpyHostToDevice));
   return FAME_OK;
-}
-
-// theta_x, theta_y(xy), theta_z(xyz) (FAME_Main/FAME_Matrix_Lambdas.cu:43-70)
-static void thetas(const fame_lattice& L, const double* k, double th[3]) {
-  const double* a = L.lattice_vec_a;
-  auto dot = [&](const double* v) { return k[0] * v[0] + k[1] * v[1] + k[2] * v[2]; };
-  th[0] = dot(a);
-  if (L.simple) {
-    th[1] = dot(a + 3);
-    th[2] = dot(a + 6);
-    return;
-  }
-  double c1 = 0.0;
-  if (a[3] > 0)
-    c1 = -(double)L.m[0] / (double)L.grid[0];
-  else if (a[3] < 0)
-    c1 = 1. - (double)L.m[0] / (double)L.grid[0];
-  const double c2 = (double)L.m[2] / (double)L.grid[1];
-  const double c3 = (double)L.m[1] / (double)L.grid[0];
-  double a2h[3], a3h[3];
-  for (int i = 0; i < 3; i++) a2h[i] = c1 * a[i] + a[3 + i];
-  for (int i = 0; i < 3; i++) a3h[i] = a[6 + i] - c2 * a2h[i] - c3 * a[i] + L.t1[i];
-  th[1] = dot(a2h);
-  th[2] = dot(a3h);
-}
-
-static int reduced_size(const fame_lattice& L, const double* k) {
-  const int N = L.grid[0] * L.grid[1] * L.grid[2];
-  const double nrm = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
-  // Gamma point: Nd = N - 1 (…Lambdas.cu:157 Simple, threshold 1e-4; :406 General, 1e-3)
-  return nrm < (L.simple ? 1e-4 : 1e-3) ? N - 1 : N;
 }
 
 static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool mixed, bool vec) {
@@ -601,6 +524,60 @@ __global__ void __launch_bounds__(256) k_adj_grad(const double2* E, const double
   grad[(long)band * N + v] = w[band] > 0 ? -0.5 * w[band] * s / den[band] : 0.0;
 }
 
+// Sum over bands of c_i |E_i|^2 on the three edges of voxel v, with
+// c_i = -(w_i / 2) g_i / (E_i^H B E_i) (zero for w_i = 0): the vector-Jacobian
+// product sum_i g_i dw_i/deps_v.  E holds nvec bands from band `first` (the Gamma
+// point keeps the two patched zero bands off the device).
+__global__ void __launch_bounds__(256) k_adj_vjp(const double2* E, const double* wgd, int nwant, int first,
+                                                 long N, double* grad) {
+  FAME_COUNT_LAUNCH();
+  __shared__ double coef[64];
+  if (threadIdx.x < nwant) {
+    const int i = threadIdx.x;
+    const double w = wgd[i], g = wgd[nwant + i];
+    coef[i] = (i >= first && w > 0) ? -0.5 * w * g / wgd[2 * nwant + i - first] : 0.0;
+  }
+  __syncthreads();
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  double acc = 0.0;
+  for (int i = first; i < nwant; i++) {
+    const double2* e = E + (long)(i - first) * 3 * N;
+    acc += coef[i] * (cabs2(e[v]) + cabs2(e[N + v]) + cabs2(e[2 * N + v]));
+  }
+  grad[v] = acc;
+}
+
+// Edge permittivities from device memory: count and locate entries that are not
+// finite and positive (pass 0), then write B, 1/B in FP64 and FP32 and, for General
+// lattices, 1/B in the field layout (x, y, z; z fastest) of the pencil stage (pass 1).
+__global__ void __launch_bounds__(256) k_eps_device(Geom g, const double* B, int pass, int* bad, double* B64,
+                                                    double* ib64, float* ib32, double* ib64q, float* ib32q) {
+  FAME_COUNT_LAUNCH();
+  const long n3 = 3L * g.N;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (long)gridDim.x * blockDim.x) {
+    const double b = B[e];
+    if (pass == 0) {
+      if (!(b > 0.0) || !isfinite(b)) {
+        atomicAdd(bad, 1);
+        atomicMin(bad + 1, (int)e);
+      }
+      continue;
+    }
+    const double ib = 1.0 / b;
+    B64[e] = b;
+    ib64[e] = ib;
+    ib32[e] = (float)ib;
+    if (g.general) {
+      const long comp = e / g.N, r = e - comp * g.N;
+      const long x = r % g.Nx, y = (r / g.Nx) % g.Ny, z = r / ((long)g.Nx * g.Ny);
+      const long q = comp * g.N + (x * g.Ny + y) * g.Nz + z;
+      ib64q[q] = ib;
+      ib32q[q] = (float)ib;
+    }
+  }
+}
+
 // ------------------------------------------------------------------ recording
 struct SolveCfg {
   int nslots, nstep, nwant, es_maxit, ls_maxit, mixed, vec, inner_maxit;
@@ -621,7 +598,7 @@ static std::string cfg_key(const SolveCfg& s, bool graph) {
 // Lanczos vector u_j of every live slot, leaving w in U[:, j+1]; then one Lanczos step.
 // device ints of the loop conditions: flag of loop i at flags[i], its trip counter
 // and overflow marker at flags[kTrips + 2i]
-constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopNone = 3, kLoopRestart = 4, kTrips = 32;
+constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopRestart = 4, kTrips = 32;
 static Cond loop_cond(Program& P, int* flags, int id, int cap, int loop_cap = 0) {
   return P.make_cond(flags + id, flags + kTrips + 2 * id, loop_cap > 0 ? std::min(cap, loop_cap) : cap);
 }
@@ -838,8 +815,9 @@ void fame_ctx_destroy(fame_ctx* c) {
     b->release();
   for (auto* b : {&c->r32, &c->x32, &c->p32, &c->T32, &c->tw32}) b->release();
   for (auto* b : {&c->invB64, &c->invB64q, &c->B64, &c->partials, &c->T0, &c->T1, &c->hcoef, &c->theta, &c->Z, &c->G,
-                  &c->stats})
+                  &c->stats, &c->adj})
     b->release();
+  c->eps_bad.release();
   c->invB32.release();
   c->invB32q.release();
   c->slots.release();
@@ -941,16 +919,23 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     set_err("invalid solver parameters (need 1 <= nwant < nstep <= 64, positive tolerances)");
     return FAME_ERR_BAD_INPUT;
   }
-  if (p.want_vectors && !evec_out) {
-    set_err("want_vectors set but evec_out is NULL");
+  const bool vec_device = p.want_vectors && !evec_out;  // eigenvectors kept on the device
+  if (vec_device && p.batch > 0 && p.batch < nk) {
+    set_err("eigenvectors kept on the device (evec_out NULL) need all k-points in one batch");
     return FAME_ERR_BAD_INPUT;
   }
+  c->dev_vec_nk = 0;
   int rc_all = FAME_OK;
   int status_any = 0;
   try {
     FAME_CK(cudaSetDevice(c->device));
     SolveCfg s;
     s.nslots = choose_batch(c, nk, &p, p.want_vectors || resabs_out);
+    if (vec_device && s.nslots < nk) {
+      set_err("eigenvectors kept on the device (evec_out NULL) need all k-points in one batch; " +
+              std::to_string(nk) + " k-points exceed the " + std::to_string(s.nslots) + " that fit");
+      return FAME_ERR_BAD_INPUT;
+    }
     s.nstep = p.nstep;
     s.nwant = p.nwant;
     s.es_maxit = p.es_maxit;
@@ -991,10 +976,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
         memset(&sl, 0, sizeof(sl));
         if (q < nb) {
           const double* k = k_xyz + 3L * (b0 + q);
-          thetas(c->lat, k, sl.th);
-          sl.Nd = reduced_size(c->lat, k);
-          sl.off = (int)N - sl.Nd;
-          sl.active = 1;
+          sl = make_slot(c->lat, k);
         } else {
           sl.Nd = (int)N;
           sl.active = 0;
@@ -1074,7 +1056,14 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
         }
         if (status[q] != 0) rc_all = FAME_ERR_NO_CONVERGENCE;
         status_any |= status[q];
-        if (s.vec) {
+        if (s.vec && vec_device) {
+          if (q == 0) {
+            c->dev_vec_nk = nb;
+            c->dev_vec_nwant = s.nwant;
+            c->dev_vec_gamma.assign(nb, 0);
+          }
+          c->dev_vec_gamma[q] = gamma ? 1 : 0;
+        } else if (s.vec) {
           const size_t n3 = 3 * (size_t)N;
           double2* dst = reinterpret_cast<double2*>(evec_out) + (size_t)kk * s.nwant * n3;
           const double2* src = c->E.p + (size_t)q * s.nwant * n3;
@@ -1125,12 +1114,7 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
     FAME_CK(cudaSetDevice(c->device));
     ensure_workspace(c, 1, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), c->cap_mixed, c->cap_vec);
     if (precision == FAME_MIXED) ensure_workspace(c, 1, c->cap_nstep, c->cap_nwant, true, c->cap_vec);
-    Slot sl;
-    memset(&sl, 0, sizeof(sl));
-    thetas(c->lat, k, sl.th);
-    sl.Nd = reduced_size(c->lat, k);
-    sl.off = c->g.N - sl.Nd;
-    sl.active = 1;
+    const Slot sl = make_slot(c->lat, k);
     if (Nd_out) *Nd_out = sl.Nd;
     FAME_CK(cudaMemcpyAsync(c->slots.p, &sl, sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
     Program P(c->stream, false, c->hflag, 100000);
@@ -1248,6 +1232,76 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
 
 void* fame_ctx_stream(fame_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
+int fame_set_option(fame_ctx* c, const char* name, int value) {
+  if (!c || !name) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const std::string n(name);
+  const bool threads_ok = value == 0 || (value >= 64 && value <= kPlaneThreads && value % 32 == 0);
+  if (n == "prefetch" && (value == 0 || value == 1)) {
+    c->prefetch = value;
+  } else if (n == "radix_order" && value >= 0 && value < kNumRadixOrders) {
+    Geom g;
+    std::string err;
+    if (layout_geom(c->lat, g, 1L << 28, err, value) != FAME_OK || geom_level(g) != c->rare) {
+      set_err("radix order " + std::to_string(value) + " gives no plan for this grid");
+      return FAME_ERR_BAD_INPUT;
+    }
+    c->radix_order = value;
+    c->g.pf = g.pf;
+    c->g.pm = g.pm;
+    c->g.ps = g.ps;
+  } else if (n == "plane_threads32" && threads_ok) {
+    c->threads32_opt = value;
+    c->plane_threads32 = value ? value : plane_threads_rule<float>(c->g, c->rare);
+  } else if (n == "plane_threads64" && threads_ok) {
+    c->threads64_opt = value;
+    c->plane_threads = value ? value : plane_threads_rule<double>(c->g, c->rare);
+  } else {
+    set_err("unknown option or value: " + n + " = " + std::to_string(value));
+    return FAME_ERR_BAD_INPUT;
+  }
+  c->progs.clear();  // recorded graphs carry the old launch parameters
+  c->waves.clear();
+  return FAME_OK;
+}
+
+int fame_get_option(fame_ctx* c, const char* name, int* value) {
+  if (!c || !name || !value) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  const std::string n(name);
+  if (n == "prefetch") {
+    *value = c->prefetch;
+  } else if (n == "radix_order") {
+    *value = c->radix_order;
+  } else if (n == "plane_threads32") {
+    *value = c->plane_threads32;
+  } else if (n == "plane_threads64") {
+    *value = c->plane_threads;
+  } else if (n == "static96") {
+    *value = c->stat96 ? 1 : 0;
+  } else if (n == "general") {
+    *value = c->g.general;
+  } else if (n == "grid_x" || n == "grid_y" || n == "grid_z") {
+    *value = n == "grid_x" ? c->g.Nx : n == "grid_y" ? c->g.Ny : c->g.Nz;
+  } else if (n == "level") {
+    *value = c->rare;
+  } else if (n == "plan_signature") {
+    // the radix lists of the three axis plans, hashed (equal plans, equal values)
+    unsigned h = 2166136261u;
+    for (const AxisPlan* a : {&c->g.pf, &c->g.pm, &c->g.ps})
+      for (int i = 0; i < a->npass; i++) h = (h ^ (unsigned)a->radix[i]) * 16777619u;
+    *value = (int)(h & 0x7fffffff);
+  } else {
+    set_err("unknown option: " + n);
+    return FAME_ERR_BAD_INPUT;
+  }
+  return FAME_OK;
+}
+
 int fame_set_loop_cap(fame_ctx* c, int max_trips) {
   if (!c || max_trips < 0) {
     set_err("null context or negative loop cap");
@@ -1293,12 +1347,7 @@ int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, int nb
     FAME_CK(cudaSetDevice(c->device));
     ensure_workspace(c, nbatch, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), precision == FAME_MIXED,
                      c->cap_vec);
-    Slot sl;
-    memset(&sl, 0, sizeof(sl));
-    thetas(c->lat, k, sl.th);
-    sl.Nd = reduced_size(c->lat, k);
-    sl.off = c->g.N - sl.Nd;
-    sl.active = 1;
+    const Slot sl = make_slot(c->lat, k);
     std::vector<Slot> hs(nbatch, sl);  // the same k-point in every slot of the batch
     FAME_CK(cudaMemcpyAsync(c->slots.p, hs.data(), nbatch * sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
     Program P(c->stream, false, c->hflag, 1);
@@ -1349,6 +1398,174 @@ int fame_bench_qbq(fame_ctx* c, const double* k, int precision, int reps, int nb
     *ms_out = (tot[0] + tot[1] + tot[2]) / reps;
     if (stage_ms)
       for (int q = 0; q < 3; q++) stage_ms[q] = tot[q] / reps;
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  return FAME_OK;
+}
+
+int fame_bench_cg(fame_ctx* c, const double* k, int reps, int nbatch, double* ms_out, double* stage_ms) {
+  if (!c || !k || !ms_out || reps < 1 || nbatch < 1 || nbatch > 64) {
+    set_err("bad argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (!c->have_eps) {
+    set_err("permittivity not set");
+    return FAME_ERR_BAD_INPUT;
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    ensure_workspace(c, nbatch, std::max(2, c->cap_nstep), std::max(1, c->cap_nwant), true, c->cap_vec);
+    const Slot sl = make_slot(c->lat, k);
+    std::vector<Slot> hs(nbatch, sl);
+    FAME_CK(cudaMemcpyAsync(c->slots.p, hs.data(), nbatch * sizeof(Slot), cudaMemcpyHostToDevice, c->stream));
+    const Geom& g = c->g;
+    const long M = 2L * g.N, F = 3L * g.N;
+    // r: a fixed pseudo-random residual; p = x = 0; the first iteration takes p = r
+    std::vector<float2> hr((size_t)nbatch * M);
+    unsigned long long z = 0x9e3779b97f4a7c15ull;
+    for (auto& v : hr) {
+      z = z * 6364136223846793005ull + 1442695040888963407ull;
+      v.x = (float)((double)(z >> 11) / 9007199254740992.0 - 0.5);
+      z = z * 6364136223846793005ull + 1442695040888963407ull;
+      v.y = (float)((double)(z >> 11) / 9007199254740992.0 - 0.5);
+    }
+    FAME_CK(cudaMemcpyAsync(c->r32.p, hr.data(), hr.size() * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    FAME_CK(cudaMemsetAsync(c->x32.p, 0, (size_t)nbatch * M * sizeof(float2), c->stream));
+    FAME_CK(cudaMemsetAsync(c->p32.p, 0, (size_t)nbatch * M * sizeof(float2), c->stream));
+    std::vector<CgState> cs(nbatch);
+    for (auto& s : cs) {
+      memset(&s, 0, sizeof(s));
+      s.iter = 1;
+      s.active = 1;
+      s.maxit = 1 << 30;
+      s.r1 = 1.0;
+      s.tol2 = 0.0;
+    }
+    FAME_CK(cudaMemcpyAsync(c->cg.p, cs.data(), nbatch * sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
+    Program P(c->stream, false, c->hflag, 1);
+    Ops o{c, P, nbatch};
+    const int tmax = std::max({g.Nx * g.Ny, g.Nx, g.Ny, g.Nz});
+    P.launch(k_tables, dim3((tmax + 255) / 256, nbatch), dim3(256), 0, g, (const Slot*)c->slots.p, c->tabs.p,
+             (double)c->lat.m[0], (double)c->lat.m[1], (double)c->lat.m[2]);
+    DBuf<unsigned char> flush;
+    const size_t fl = 256ull << 20;
+    flush.ensure(fl);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) FAME_CK(cudaEventCreate(&e));
+    double tot[3] = {0, 0, 0};
+    for (int it = 0; it < reps + 1; it++) {
+      FAME_CK(cudaMemsetAsync(flush.p, it & 0xff, fl, c->stream));
+      FAME_CK(cudaEventRecord(ev[0], c->stream));
+      o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr, Cond{},
+                                       c->x32.p);
+      FAME_CK(cudaEventRecord(ev[1], c->stream));
+      o.pencil<float, PEN_QBQ_CG>(c->T32.p, 1, F, c->ibq32(), 1);
+      FAME_CK(cudaEventRecord(ev[2], c->stream));
+      o.plane_fwd<float, EPI_CGR, false>(c->T32.p, nullptr, 1, M, F, nullptr, nullptr, Cond{}, 0.0, c->r32.p);
+      FAME_CK(cudaEventRecord(ev[3], c->stream));
+      FAME_CK(cudaEventSynchronize(ev[3]));
+      if (it == 0) continue;  // warm-up (the p = r iteration)
+      for (int q = 0; q < 3; q++) {
+        float ms = 0;
+        FAME_CK(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+        tot[q] += ms;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    flush.release();
+    *ms_out = (tot[0] + tot[1] + tot[2]) / reps;
+    if (stage_ms)
+      for (int q = 0; q < 3; q++) stage_ms[q] = tot[q] / reps;
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  return FAME_OK;
+}
+
+int fame_set_eps_device(fame_ctx* c, const double* B) {
+  if (!c || !B) {
+    set_err("null argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    c->eps_bad.ensure(2);
+    const int init[2] = {0, 0x7fffffff};
+    FAME_CK(cudaMemcpyAsync(c->eps_bad.p, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+    const Geom& g = c->g;
+    const int blocks = (int)std::min<long>(4096, (3L * g.N + 255) / 256);
+    k_eps_device<<<blocks, 256, 0, c->stream>>>(g, B, 0, c->eps_bad.p, nullptr, nullptr, nullptr, nullptr, nullptr);
+    FAME_CK(cudaGetLastError());
+    int bad[2];
+    FAME_CK(cudaMemcpyAsync(bad, c->eps_bad.p, sizeof(bad), cudaMemcpyDeviceToHost, c->stream));
+    FAME_CK(cudaStreamSynchronize(c->stream));
+    if (bad[0]) {
+      set_err("permittivity must be finite and positive (" + std::to_string(bad[0]) + " edges, first " +
+              std::to_string(bad[1]) + ")");
+      return FAME_ERR_BAD_INPUT;
+    }
+    k_eps_device<<<blocks, 256, 0, c->stream>>>(g, B, 1, c->eps_bad.p, c->B64.p, c->invB64.p, c->invB32.p,
+                                                  c->invB64q.p, c->invB32q.p);
+    FAME_CK(cudaGetLastError());
+    FAME_CK(cudaStreamSynchronize(c->stream));
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  c->have_eps = true;
+  return FAME_OK;
+}
+
+int fame_adjoint_vjp(fame_ctx* c, int kidx, const double* freq, const double* grad_w, int nwant, double rel_gap,
+                     double* grad_dev) {
+  if (!c || !freq || !grad_w || !grad_dev || nwant < 1 || nwant > 64 || !(rel_gap >= 0)) {
+    set_err("null argument, nwant outside 1..64 or negative gap");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (kidx < 0 || kidx >= c->dev_vec_nk || nwant != c->dev_vec_nwant) {
+    set_err("no eigenvectors of this k-point on the device (solve with want_vectors and evec_out NULL first)");
+    return FAME_ERR_BAD_INPUT;
+  }
+  // degenerate groups: a derivative of one band of a group is not defined, the sum
+  // over the group is; so the weights of a group's bands must be equal
+  double gmax = 0;
+  for (int i = 0; i < nwant; i++) gmax = std::max(gmax, fabs(grad_w[i]));
+  for (int i = 0; i < nwant; i++)
+    for (int j = i + 1; j < nwant; j++) {
+      const double wi = freq[i], wj = freq[j];
+      if (wi <= 0 || wj <= 0) continue;
+      if (fabs(wi - wj) <= rel_gap * std::max(wi, wj) && fabs(grad_w[i] - grad_w[j]) > 1e-12 * gmax) {
+        set_err("bands " + std::to_string(i) + " and " + std::to_string(j) +
+                " are degenerate (relative gap below " + std::to_string(rel_gap) +
+                ") but weighted differently; the derivative of one band of a degenerate group is not defined, "
+                "weight the whole group equally");
+        return FAME_ERR_BAD_INPUT;
+      }
+    }
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    const long N = c->g.N;
+    const int gamma = c->dev_vec_gamma[kidx];
+    const int first = gamma ? 2 : 0;
+    const int nvec = nwant - first;
+    const double2* E = c->E.p + (size_t)kidx * nwant * 3 * N;
+    c->adj.ensure(3 * 64);
+    std::vector<double> wg(2 * nwant);
+    for (int i = 0; i < nwant; i++) {
+      wg[i] = freq[i];
+      wg[nwant + i] = grad_w[i];
+    }
+    FAME_CK(cudaMemcpyAsync(c->adj.p, wg.data(), wg.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (nvec > 0) {
+      k_adj_den<<<nvec, 1024, 0, c->stream>>>(E, c->B64.p, 3 * N, c->adj.p + 2 * nwant);
+      FAME_CK(cudaGetLastError());
+    }
+    k_adj_vjp<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(E, c->adj.p, nwant, first, N, grad_dev);
+    FAME_CK(cudaGetLastError());
+    FAME_CK(cudaStreamSynchronize(c->stream));
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;

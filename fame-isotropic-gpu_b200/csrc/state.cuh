@@ -126,6 +126,8 @@ struct PlaneInArgs {
   int sigma;              // IN_VEC: multiply the input by sqrt(Lambda_q) first (Sigma, …_Isotropic.cu:109)
   cplx<R>* T;             // output field (3 components)
   Cond reset;             // loop condition cleared by this kernel when it starts a loop body
+  int pf_dist;            // > 0: each CTA prefetches into L2 the operands of the CTA this
+                          // many places later in launch order (about one wave ahead)
 };
 
 template <typename R>
@@ -147,6 +149,7 @@ struct PencilArgs {
   unsigned* counters;      // PEN_QBQ_CG: [nslots] ticket counters
   int TW;                  // fast positions per CTA
   int nslots;              // k-points of the launch (k_pencil_pipe walks all their tiles)
+  int pf_dist;             // > 0: L2 prefetch of the tile of the CTA this many places later
 };
 
 template <typename R>
@@ -168,6 +171,7 @@ struct PlaneOutArgs {
   Cond cond;               // EPI_RESID: outer WHILE condition; EPI_CGR: CG WHILE condition
   int nslots;
   double tol2;             // EPI_RESID: absolute tolerance^2 on ||b - A y||
+  int pf_dist;             // > 0: L2 prefetch of the operands of the CTA this many places later
 };
 
 }  // namespace fame

@@ -30,7 +30,9 @@ OP_QR, OP_QRS, OP_QBQ, OP_PR, OP_PRS, OP_INVAR = range(6)
 EXPORTS = ("fame_ctx_create", "fame_ctx_destroy", "fame_set_eps", "fame_set_material", "fame_solve_kpoints",
            "fame_apply", "fame_adjoint", "fame_ctx_sizes", "fame_last_error", "fame_version", "fame_ctx_stream",
            "fame_launch_count", "fame_bench_qbq", "fame_qbq_static", "fame_material_locate",
-           "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish", "fame_set_loop_cap")
+           "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish", "fame_set_loop_cap",
+           "fame_bench_cg", "fame_set_eps_device", "fame_adjoint_vjp", "fame_set_option", "fame_get_option",
+           "fame_tune")
 # fame_kcounters.detail bits (FAME_KSTATUS_*)
 KSTATUS_QL, KSTATUS_LANCZOS, KSTATUS_CG = 1, 2, 4
 QBQ_STATIC_SCRATCH_BYTES = 4 << 20  # FAME_QBQ_STATIC_SCRATCH_BYTES
@@ -104,12 +106,19 @@ def load():
     lib.fame_writer_start.argtypes = [C.c_char_p, D, C.c_int, C.c_longlong, C.c_int, C.c_int, C.POINTER(P)]
     lib.fame_writer_finish.argtypes = [P]
     lib.fame_set_loop_cap.argtypes = [P, C.c_int]
+    lib.fame_bench_cg.argtypes = [P, D, C.c_int, C.c_int, D, D]
+    lib.fame_set_eps_device.argtypes = [P, P]
+    lib.fame_adjoint_vjp.argtypes = [P, C.c_int, D, D, C.c_int, C.c_double, P]
+    lib.fame_set_option.argtypes = [P, C.c_char_p, C.c_int]
+    lib.fame_get_option.argtypes = [P, C.c_char_p, C.POINTER(C.c_int)]
+    lib.fame_tune.argtypes = [P, D, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
     lib.fame_last_error.restype = C.c_char_p
     lib.fame_version.restype = C.c_char_p
     for fn in ("fame_ctx_create", "fame_set_eps", "fame_set_material", "fame_solve_kpoints", "fame_apply",
                "fame_adjoint", "fame_ctx_sizes", "fame_launch_count", "fame_bench_qbq", "fame_qbq_static",
                "fame_material_locate", "fame_write_eigenvectors", "fame_writer_start", "fame_writer_finish",
-               "fame_set_loop_cap"):
+               "fame_set_loop_cap", "fame_bench_cg", "fame_set_eps_device", "fame_adjoint_vjp",
+               "fame_set_option", "fame_get_option", "fame_tune"):
         getattr(lib, fn).restype = C.c_int
     _lib = lib
     return lib
@@ -209,22 +218,38 @@ class Context:
         assert B.size == 3 * self.N
         _check(load().fame_set_eps(self._h, _dptr(B)))
 
+    def set_eps_device(self, B):
+        """Edge permittivities from a contiguous float64 CUDA tensor of 3N values on the
+        context's device (stays on the GPU)."""
+        import torch
+        _check_device_tensor(B, "B", torch.float64, 3 * self.N, self.device)
+        _check(load().fame_set_eps_device(self._h, C.c_void_p(B.data_ptr())))
+
     def set_material(self, binout, material_num, eps_in, eps_out):
         b = np.ascontiguousarray(binout, dtype=np.int32)
         e = np.ascontiguousarray(eps_in, dtype=np.float64)
         _check(load().fame_set_material(self._h, b.ctypes.data_as(C.POINTER(C.c_int)), int(material_num),
                                         _dptr(e), float(eps_out)))
 
-    def solve(self, kpoints, params=None, resabs=False, **kw):
+    def solve(self, kpoints, params=None, resabs=False, vectors_on_device=False, **kw):
         """Returns dict(freq, relres, relerr, counters[, resabs][, evec]) for kpoints (nk, 3).
-        resabs: also the residual norm of E scaled as the reference restores it."""
+        resabs: also the residual norm of E scaled as the reference restores it.
+        vectors_on_device: keep the eigenvectors on the GPU (for adjoint_vjp) instead of
+        returning them; all k-points then run as one batch."""
         p = params or solver_params(**kw)
+        if vectors_on_device:
+            q = SolverParams()
+            C.memmove(C.byref(q), C.byref(p), C.sizeof(SolverParams))
+            q.want_vectors = 1
+            p = q
+        self.solves = getattr(self, "solves", 0) + 1
         k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
         nk = k.shape[0]
         freq = np.zeros((nk, p.nwant))
         rr = np.zeros((nk, p.nwant))
         re = np.zeros((nk, p.nwant))
-        ev = np.zeros((nk, p.nwant, 3 * self.N), dtype=np.complex128) if p.want_vectors else None
+        ev = np.zeros((nk, p.nwant, 3 * self.N), dtype=np.complex128) if p.want_vectors and not vectors_on_device \
+            else None
         cnt = (KCounters * nk)()
         ra = np.zeros((nk, p.nwant)) if resabs else None
         rc = load().fame_solve_kpoints(self._h, _dptr(k), nk, C.byref(p), _dptr(freq), _dptr(rr), _dptr(re),
@@ -265,6 +290,24 @@ class Context:
         a loop that reaches it ends the solve with ERR_WATCHDOG."""
         _check(load().fame_set_loop_cap(self._h, int(max_trips)))
 
+    def set_option(self, name, value):
+        """Execution option of the context (fame_set_option)."""
+        _check(load().fame_set_option(self._h, name.encode(), int(value)))
+
+    def get_option(self, name):
+        v = C.c_int()
+        _check(load().fame_get_option(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def tune(self, k, precision=MIXED, batch=1, cache_file=None):
+        """FFT plan autotuner (fame_tune): times candidate plans, applies the fastest
+        and returns it as text; cache_file keeps winners across runs."""
+        kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+        buf = C.create_string_buffer(256)
+        cf = None if cache_file is None else os.fsencode(cache_file)
+        _check(load().fame_tune(self._h, _dptr(kk), int(precision), int(batch), cf, buf, 256))
+        return buf.value.decode()
+
     def stream(self):
         """The context's cudaStream_t as an int (for torch.cuda.ExternalStream)."""
         return load().fame_ctx_stream(self._h)
@@ -283,6 +326,31 @@ class Context:
         _check(load().fame_bench_qbq(self._h, _dptr(kk), int(precision), int(reps), int(nbatch), C.byref(ms),
                                      _dptr(st)))
         return ms.value, st
+
+    def bench_cg(self, k, reps=20, nbatch=1):
+        """Mean device ms of one FP32 CG iteration (its three kernels, L2 flushed
+        before each) on a batch of nbatch k-points, and of each kernel."""
+        kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+        ms = C.c_double()
+        st = np.zeros(3)
+        _check(load().fame_bench_cg(self._h, _dptr(kk), int(reps), int(nbatch), C.byref(ms), _dptr(st)))
+        return ms.value, st
+
+    def adjoint_vjp(self, kidx, freq, grad_w, rel_gap=1e-6, out=None):
+        """sum_i grad_w[i] d(omega_i)/d(eps_voxel) as a float64 CUDA tensor (N,) on the
+        context's device, for k-point kidx of the last solve(vectors_on_device=True).
+        Degenerate groups (relative gap <= rel_gap) must carry equal weights."""
+        import torch
+        f = np.ascontiguousarray(freq, dtype=np.float64).reshape(-1)
+        g = np.ascontiguousarray(grad_w, dtype=np.float64).reshape(-1)
+        if f.size != g.size:
+            raise ValueError("freq and grad_w differ in length")
+        if out is None:
+            out = torch.empty(self.N, dtype=torch.float64, device=f"cuda:{self.device}")
+        _check_device_tensor(out, "out", torch.float64, self.N, self.device)
+        _check(load().fame_adjoint_vjp(self._h, int(kidx), _dptr(f), _dptr(g), f.size, float(rel_gap),
+                                       C.c_void_p(out.data_ptr())))
+        return out
 
     def adjoint(self, freq, evec):
         """d(omega_i)/d(eps_voxel) for one k: freq (nwant,), evec (nwant, 3N) complex128 host."""

@@ -19,10 +19,38 @@ def shard_bounds(nk: int, world_size: int, rank: int) -> tuple[int, int]:
     return nk * rank // world_size, nk * (rank + 1) // world_size
 
 
-def solve_sharded(ctx, kpoints, params, group=None, resabs=False):
+def balanced_bounds(costs, world_size: int) -> list[tuple[int, int]]:
+    """Contiguous blocks [start, stop), one per rank, cut where the running sum of the
+    per-k costs crosses r / world_size of the total (each cut at the nearer side of the
+    crossing), so no block exceeds its share by more than one k-point's cost.  Uniform
+    costs give blocks whose sizes differ by at most one.  Costs are e.g. a previous solve's CG iterations per
+    k-point (the work of a k-point is its CG iterations times the operator cost, which is
+    the same for every k-point of a grid)."""
+    c = np.asarray(costs, dtype=np.float64).reshape(-1)
+    if world_size < 1 or np.any(c < 0):
+        raise ValueError("bad world size or negative cost")
+    nk = c.size
+    if nk == 0 or not np.any(c > 0):
+        return [shard_bounds(nk, world_size, r) for r in range(world_size)]
+    pre = np.concatenate([[0.0], np.cumsum(c)])
+    tot = pre[-1]
+    cuts = [0]
+    for r in range(1, world_size):
+        t = tot * r / world_size
+        i = int(np.searchsorted(pre, t))  # pre[i-1] < t <= pre[i]
+        i = min(max(i, 1), nk)
+        if t - pre[i - 1] < pre[i] - t:
+            i -= 1
+        cuts.append(max(cuts[-1], min(i, nk)))
+    cuts.append(nk)
+    return [(cuts[r], cuts[r + 1]) for r in range(world_size)]
+
+
+def solve_sharded(ctx, kpoints, params, group=None, resabs=False, costs=None):
     """Solves this rank's block of `kpoints` (nk, 3) on its own context and gathers
     every block to every rank.  Returns dict(freq, relres, relerr, counters[, resabs])
-    for all nk k-points in input order.  Without an initialised process group it
+    for all nk k-points in input order.  costs (nk values, or None for equal costs)
+    balance the blocks (balanced_bounds).  Without an initialised process group it
     solves everything locally."""
     import torch.distributed as dist
 
@@ -32,7 +60,7 @@ def solve_sharded(ctx, kpoints, params, group=None, resabs=False):
         return ctx.solve(k, params, resabs=resabs)
     ws = dist.get_world_size(group)
     rank = dist.get_rank(group)
-    a, b = shard_bounds(nk, ws, rank)
+    a, b = shard_bounds(nk, ws, rank) if costs is None else balanced_bounds(costs, ws)[rank]
     part = None
     if b > a:
         out = ctx.solve(k[a:b], params, resabs=resabs)

@@ -114,12 +114,16 @@ int fame_set_material(fame_ctx* ctx, const int* binout, int material_num, const 
  *   freq_out   nk*nwant   omega = sqrt(1/theta) per band (FAME_Fast_Algorithms_Isotropic.cu
  *                         + Lanczos_Isotropic.cu:88, Gamma patch :61-79);
  *   relres_out nk*nwant   ||C^H C E - w^2 B E|| / (w^2 ||B E||) evaluated in FP64, or NULL;
- *   relerr_out nk*nwant   |w^2 - rho| / rho with rho the FP64 Rayleigh quotient, or NULL;
+ *   relerr_out nk*nwant   |w^2 - rho| / rho with rho the FP64 Rayleigh quotient of the
+ *                         band's own Ritz vector (the library's FP64 check of each
+ *                         eigenvalue; not a comparison with a separate FP64 solve), or NULL;
  *   resabs_out nk*nwant   ||C^H C E - w^2 B E|| for E scaled as the reference restores it
  *                         (FAME_Fast_Algorithms_Isotropic.cu:119-121), the quantity its
  *                         Check_Residual tests against 1e-10 (FAME_Main_Code.cu:383-421),
  *                         or NULL (non-NULL adds one Q_r apply per band);
- *   evec_out   nk*nwant*3N complex128 (params->want_vectors), or NULL;
+ *   evec_out   nk*nwant*3N complex128 (params->want_vectors), or NULL: with
+ *              want_vectors set and evec_out NULL the eigenvectors stay on the device
+ *              for fame_adjoint_vjp (all nk k-points must fit one batch);
  *   counters   nk entries, or NULL.
  * Replaces FAME_Fast_Algorithms_Driver (FAME_Main/FAME_Main_Code.cu:142-171) over
  * the k-loop of FAME_Main_Code (:79-133). */
@@ -143,6 +147,25 @@ int fame_apply(fame_ctx* ctx, int op, const double* k_xyz, const void* in, void*
 int fame_adjoint(fame_ctx* ctx, const double* freq, const double* evec, int nwant, int host,
                  double* grad_out);
 
+/* Edge permittivities B (3N doubles) in DEVICE memory of the context's device, for
+ * callers that keep the permittivity on the GPU (inverse design).  Entries that are
+ * not finite and positive are rejected with FAME_ERR_BAD_INPUT before anything is
+ * written.  Same effect as fame_set_eps otherwise. */
+int fame_set_eps_device(fame_ctx* ctx, const double* B_eps_device);
+
+/* Vector-Jacobian product of the band frequencies for one k-point of the last
+ * fame_solve_kpoints call that kept its eigenvectors on the device (want_vectors set,
+ * evec_out NULL, all k-points in one batch): grad_device[v] = sum_i grad_w[i]
+ * dw_i/deps_v for one permittivity per voxel (the Hellmann-Feynman form of
+ * fame_adjoint), written to N doubles of device memory.  freq and grad_w are the
+ * nwant frequencies of that k-point and their weights (host).  Bands whose relative
+ * gap is at most rel_gap form degenerate groups: the derivative of a single band of a
+ * group is not defined, so unequal weights inside a group are FAME_ERR_BAD_INPUT;
+ * equal weights give the derivative of the group's sum.  No counterpart in the
+ * reference, which has no adjoint. */
+int fame_adjoint_vjp(fame_ctx* ctx, int kidx, const double* freq, const double* grad_w, int nwant,
+                     double rel_gap, double* grad_device);
+
 /* The context's CUDA stream (a cudaStream_t), so callers can time work on it with
  * CUDA events.  All device work of the context runs on this stream. */
 void* fame_ctx_stream(fame_ctx* ctx);
@@ -159,6 +182,33 @@ int fame_launch_count(fame_ctx* ctx, unsigned long long* count_out);
  * reference, whose loops are host-driven. */
 int fame_set_loop_cap(fame_ctx* ctx, int max_trips);
 
+/* Execution options of a context, used by later solves and operator applies (they
+ * change how the kernels run; the results agree to rounding):
+ *   "prefetch"         1: each CTA of the mixed-precision CG's stage kernels issues L2
+ *                      prefetches of the operands of the CTA one wave later; 0 (default): none.
+ *   "radix_order"      0..3: radix order of the FFT plans of runtime-geometry grids
+ *                      (every grid but the compile-time 96^3 one); 0 is the default.
+ *   "plane_threads32", "plane_threads64": threads of a runtime-geometry plane CTA in the
+ *                      FP32 / FP64 kernels, a multiple of 32 in 64..512, or 0 for the
+ *                      built-in rule.
+ * Read-only (fame_get_option): "static96", "general", "grid_x", "grid_y", "grid_z",
+ * "level" (the FFT pass level the grid needs).  fame_tune picks these options by timing.
+ * Unknown names or values are FAME_ERR_BAD_INPUT.  No counterpart in the reference. */
+int fame_set_option(fame_ctx* ctx, const char* name, int value);
+int fame_get_option(fame_ctx* ctx, const char* name, int* value);
+
+/* FFT plan autotuner: picks the execution options above ("radix_order",
+ * "plane_threads32"/"plane_threads64", "prefetch") for this context's grid by timing
+ * candidates on `batch` copies of wave vector k (CUDA events, L2 flushed before each
+ * repetition): one FP32 CG iteration for FAME_MIXED, one FP64 Q_r^* B^-1 Q_r apply for
+ * FAME_FP64.  The winner is applied to the context.  cache_file (or NULL): a text
+ * file of "key | plan" lines, key = grid, lattice family, precision and batch; a
+ * cached plan is applied without timing, a new one is appended.  plan_out (or NULL)
+ * receives the plan as text.  Replaces the fixed cuFFT plans of the reference
+ * (FAME_Main/FAME_Create_cublas.cu:16-25). */
+int fame_tune(fame_ctx* ctx, const double* k, int precision, int batch, const char* cache_file, char* plan_out,
+              int plan_len);
+
 /* Operator benchmark: `reps` applications of Q_r^* B^-1 Q_r at wave vector k in
  * FP64 (precision FAME_FP64) or FP32 (FAME_MIXED) to a batch of `nbatch` vectors
  * (1..64, the k-point repeated in every slot, as the solver batches k-points), each
@@ -168,6 +218,16 @@ int fame_set_loop_cap(fame_ctx* ctx, int max_trips);
  * stage over the whole batch; ms_out the mean of their sum. */
 int fame_bench_qbq(fame_ctx* ctx, const double* k, int precision, int reps, int nbatch, double* ms_out,
                    double* stage_ms_out);
+
+/* CG-iteration benchmark: `reps` iterations of the mixed-precision solve's FP32 CG
+ * (the three kernels of one iteration: search direction and solution update with
+ * the 2 -> 3 mix and the inverse plane transforms; slow-axis transforms with <p, Ap>;
+ * forward plane transforms with the 3 -> 2 unmix, r -= a Ap and ||r||^2) on `nbatch`
+ * k-points (1..64, the k-point repeated), from a fixed pseudo-random residual, each
+ * iteration preceded by an L2 flush outside the timed span.  stage_ms_out[3]
+ * (optional) receives the mean time of the three kernels over the batch, ms_out
+ * their sum.  The CG iteration of FAME_Main/CG.cu:36-77 on QBQ. */
+int fame_bench_cg(fame_ctx* ctx, const double* k, int reps, int nbatch, double* ms_out, double* stage_ms_out);
 
 /* Grid size N and maximum reduced size 2N of the context, for buffer sizing. */
 int fame_ctx_sizes(const fame_ctx* ctx, long long* N_out);

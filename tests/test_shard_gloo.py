@@ -15,7 +15,7 @@ import torch.distributed as dist  # noqa: E402
 import torch.multiprocessing as mp  # noqa: E402
 
 import fame_b200 as fb  # noqa: E402
-from fame_b200.shard import shard_bounds, solve_sharded  # noqa: E402
+from fame_b200.shard import balanced_bounds, shard_bounds, solve_sharded  # noqa: E402
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -42,7 +42,7 @@ def _free_port():
     return p
 
 
-def _worker(rank, ws, port, outdir, nk, fail_rank):
+def _worker(rank, ws, port, outdir, nk, fail_rank, costs=None):
     import sys
     sys.path.insert(0, ROOT)
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(ws))
@@ -54,7 +54,7 @@ def _worker(rank, ws, port, outdir, nk, fail_rank):
         p = fb.solver_params(nwant=4)
         if rank == fail_rank:
             raise RuntimeError("rank failed before the gather")
-        out = solve_sharded(FakeCtx(), k, p, resabs=True)
+        out = solve_sharded(FakeCtx(), k, p, resabs=True, costs=costs)
         ref = FakeCtx().solve(k, p, resabs=True)
         res["freq_ok"] = bool(np.array_equal(out["freq"], ref["freq"]))
         res["resabs_ok"] = bool(np.array_equal(out["resabs"], ref["resabs"]))
@@ -72,8 +72,8 @@ def _worker(rank, ws, port, outdir, nk, fail_rank):
     dist.destroy_process_group()
 
 
-def _run(tmp_path, nk, fail_rank=-1, ws=2):
-    mp.spawn(_worker, args=(ws, _free_port(), str(tmp_path), nk, fail_rank), nprocs=ws, join=True)
+def _run(tmp_path, nk, fail_rank=-1, ws=2, costs=None):
+    mp.spawn(_worker, args=(ws, _free_port(), str(tmp_path), nk, fail_rank, costs), nprocs=ws, join=True)
     return [json.load(open(tmp_path / f"rank{r}.json")) for r in range(ws)]
 
 
@@ -105,3 +105,31 @@ def test_failed_rank_ends_the_other_ranks_collective(tmp_path):
     r0, r1 = _run(tmp_path, nk=6, fail_rank=1)
     assert "rank failed" in r1["error"]
     assert "error" in r0  # the gather saw the lost peer and raised
+
+
+def test_balanced_bounds_split_by_cost():
+    rng = np.random.default_rng(2)
+    for nk in (1, 2, 7, 20, 60):
+        for ws in (1, 2, 3, 8):
+            c = rng.uniform(1.0, 3.0, nk)
+            spans = balanced_bounds(c, ws)
+            assert spans[0][0] == 0 and spans[-1][1] == nk
+            assert all(spans[i][1] == spans[i + 1][0] for i in range(ws - 1))
+            share = c.sum() / ws
+            assert max(c[a:b].sum() for a, b in spans) <= share + c.max() + 1e-9
+    # the reference's pattern on its 20-point 96^3 path: a few k-points need 1.9x the CG work
+    cost = np.array([2781, 2820, 2816, 1973, 1976, 1973, 2810, 2813, 1976, 2781,
+                     1969, 1966, 1955, 1970, 1972, 1973, 2810, 2813, 3650, 1955], float)
+    even = max(cost[a:b].sum() for a, b in (shard_bounds(20, 4, r) for r in range(4)))
+    bal = max(cost[a:b].sum() for a, b in balanced_bounds(cost, 4))
+    assert bal < even
+    sizes = [b - a for a, b in balanced_bounds(np.ones(10), 3)]
+    assert sum(sizes) == 10 and max(sizes) - min(sizes) <= 1
+
+
+def test_two_ranks_gather_with_cost_balanced_blocks(tmp_path):
+    costs = [5.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+    r0, r1 = _run(tmp_path, nk=7, costs=costs)
+    for r in (r0, r1):
+        assert "error" not in r, r
+        assert r["freq_ok"] and r["resabs_ok"] and r["counters_ok"]
