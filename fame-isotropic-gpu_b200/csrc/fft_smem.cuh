@@ -142,6 +142,86 @@ template <typename R> struct Dft<R, 8> {
   }
 };
 
+// FP32 butterflies with packed pair arithmetic (sm_100 FADD2 / FMUL2 / FFMA2: one
+// instruction updates both parts of a complex value).  Same operations and roundings
+// as the generic ones: a - b is formed as b * (-1) + a (exact product, one rounding).
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 pscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+__device__ __forceinline__ float2 pfma(float2 a, float s, float2 c) { return __ffma2_rn(a, make_float2(s, s), c); }
+
+template <> struct Dft<float, 2> {
+  __device__ __forceinline__ static void run(float2* a, bool) {
+    const float2 t = a[0];
+    a[0] = padd(t, a[1]);
+    a[1] = psub(t, a[1]);
+  }
+};
+
+template <> struct Dft<float, 3> {
+  __device__ __forceinline__ static void run(float2* a, bool inv) {
+    const float s = 0.86602540378443864676f;  // sin(2*pi/3)
+    const float2 p = padd(a[1], a[2]), q = psub(a[1], a[2]);
+    const float2 m = pfma(p, -0.5f, a[0]);
+    a[0] = padd(a[0], p);
+    // m -/+ i s q (forward) or m +/- i s q (inverse)
+    if (inv) {
+      a[1] = make_float2(m.x - s * q.y, m.y + s * q.x);
+      a[2] = make_float2(m.x + s * q.y, m.y - s * q.x);
+    } else {
+      a[1] = make_float2(m.x + s * q.y, m.y - s * q.x);
+      a[2] = make_float2(m.x - s * q.y, m.y + s * q.x);
+    }
+  }
+};
+
+template <> struct Dft<float, 4> {
+  __device__ __forceinline__ static void run(float2* a, bool inv) {
+    const float2 s0 = padd(a[0], a[2]), d0 = psub(a[0], a[2]);
+    const float2 s1 = padd(a[1], a[3]), e = psub(a[1], a[3]);
+    a[0] = padd(s0, s1);
+    a[2] = psub(s0, s1);
+    // d0 -/+ i e (forward) or d0 +/- i e (inverse)
+    if (inv) {
+      a[1] = make_float2(d0.x - e.y, d0.y + e.x);
+      a[3] = make_float2(d0.x + e.y, d0.y - e.x);
+    } else {
+      a[1] = make_float2(d0.x + e.y, d0.y - e.x);
+      a[3] = make_float2(d0.x - e.y, d0.y + e.x);
+    }
+  }
+};
+
+template <> struct Dft<float, 8> {
+  __device__ __forceinline__ static void run(float2* a, bool inv) {
+    const float h = 0.70710678118654752440f;  // 1/sqrt(2)
+    float2 e[4] = {a[0], a[2], a[4], a[6]};
+    float2 o[4] = {a[1], a[3], a[5], a[7]};
+    Dft<float, 4>::run(e, inv);
+    Dft<float, 4>::run(o, inv);
+    // twiddles w8^k, k = 1, 3 (w8 = e^{-/+ i pi/4}); k = 2 is a rotation folded below
+    const float2 x1 = o[1], x3 = o[3];
+    const float2 o1 = inv ? pscale(make_float2(x1.x - x1.y, x1.x + x1.y), h)
+                          : pscale(make_float2(x1.x + x1.y, x1.y - x1.x), h);
+    const float2 o3 = inv ? pscale(make_float2(-(x3.x + x3.y), x3.x - x3.y), h)
+                          : pscale(make_float2(x3.y - x3.x, -(x3.x + x3.y)), h);
+    a[0] = padd(e[0], o[0]);
+    a[4] = psub(e[0], o[0]);
+    a[1] = padd(e[1], o1);
+    a[5] = psub(e[1], o1);
+    const float2 y = o[2];
+    if (inv) {
+      a[2] = make_float2(e[2].x - y.y, e[2].y + y.x);
+      a[6] = make_float2(e[2].x + y.y, e[2].y - y.x);
+    } else {
+      a[2] = make_float2(e[2].x + y.y, e[2].y - y.x);
+      a[6] = make_float2(e[2].x - y.y, e[2].y + y.x);
+    }
+    a[3] = padd(e[3], o3);
+    a[7] = psub(e[3], o3);
+  }
+};
+
 // Radix 12 as a prime-factor (Good-Thomas) DFT 3 x 4, no internal twiddles:
 // input n = (4 n1 + 3 n2) mod 12, output k = (4 k1 + 9 k2) mod 12 with
 // k1 = k mod 3, k2 = k mod 4 (Chinese remainder map).

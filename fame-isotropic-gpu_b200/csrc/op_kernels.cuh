@@ -89,6 +89,16 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     }
   }
   if constexpr (IN == IN_CG) {
+    // this CTA's own r, p and x, all at once: the batched loads of the mix below then
+    // wait on one DRAM latency and find the rest in L2
+    long i0, i1;
+    if (a.self_pf && threadIdx.x < (st->iter == 1 ? 2 : 6) && plane_vec_range(P, s, comp, sl, i0, i1)) {
+      const cplx<R>* v = threadIdx.x < 2 ? a.r : threadIdx.x < 4 ? a.p : a.x;
+      const long base = (long)(slot * a.vec_per_slot + vec) * a.vstride + ((threadIdx.x & 1) ? sl.Nd : 0);
+      prefetch_l2(v + base + i0, (i1 - i0) * sizeof(cplx<R>));
+    }
+  }
+  if constexpr (IN == IN_CG) {
     // r, p and x of the CTA one wave ahead (p and x once its k-point is past k = 1)
     int x2, y2, z2;
     if (a.pf_dist > 0 && threadIdx.x < 6 && cta_of(cta_linear() + a.pf_dist, x2, y2, z2)) {
@@ -204,14 +214,22 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
           if (!first) {
             cplx<R> s1 = C1[k], s2 = C2[k];
             const cplx<R> p1 = B1[k], p2 = B2[k];
-            s1.x += are * p1.x - aim * p1.y;
-            s1.y += are * p1.y + aim * p1.x;
-            s2.x += are * p2.x - aim * p2.y;
-            s2.y += are * p2.y + aim * p2.x;
+            if constexpr (sizeof(R) == 4) {
+              // the FP32 CG's step size is real (<p, Ap> from the pencil stage): packed pairs
+              s1 = pfma(p1, are, s1);
+              s2 = pfma(p2, are, s2);
+              x1 = pfma(p1, beta, x1);
+              x2 = pfma(p2, beta, x2);
+            } else {
+              s1.x += are * p1.x - aim * p1.y;
+              s1.y += are * p1.y + aim * p1.x;
+              s2.x += are * p2.x - aim * p2.y;
+              s2.y += are * p2.y + aim * p2.x;
+              x1 = mk<R>(x1.x + beta * p1.x, x1.y + beta * p1.y);
+              x2 = mk<R>(x2.x + beta * p2.x, x2.y + beta * p2.y);
+            }
             a.x[vb + i] = s1;
             a.x[vb + Nd + i] = s2;
-            x1 = mk<R>(x1.x + beta * p1.x, x1.y + beta * p1.y);
-            x2 = mk<R>(x2.x + beta * p2.x, x2.y + beta * p2.y);
           }
           a.p[vb + i] = x1;
           a.p[vb + Nd + i] = x2;
@@ -370,7 +388,10 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
       const R ib = ibt[q];
       const cplx<R> v = tile[q];
       if constexpr (MODE == PEN_QBQ_CG) dot += (float)(ib * cabs2(v));
-      tile[q] = cscale(v, ib * invN);
+      if constexpr (sizeof(R) == 4)
+        tile[q] = pscale(v, ib * invN);
+      else
+        tile[q] = cscale(v, ib * invN);
     }
     __syncthreads();
     GP::template fft_slow_c<R, false>(tile, tws);
@@ -582,6 +603,13 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     return;
   }
   if constexpr (EPI == EPI_CGR) {
+    // this CTA's own residual, read in the epilogue: it streams into L2 during the transforms
+    long i0, i1;
+    if (a.self_pf && threadIdx.x < 2 && plane_vec_range(P, s, comp, sl, i0, i1))
+      prefetch_l2(a.r + (long)(slot * a.vec_per_slot + vec) * a.vstride + (threadIdx.x ? sl.Nd : 0) + i0,
+                  (i1 - i0) * sizeof(cplx<R>));
+  }
+  if constexpr (EPI == EPI_CGR) {
     // the field plane (4 pieces) and the residual of the CTA one wave ahead
     int x2, y2, z2;
     if (a.pf_dist > 0 && threadIdx.x < 6 && cta_of(cta_linear() + a.pf_dist, x2, y2, z2)) {
@@ -711,17 +739,25 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
         acc[0] += (double)(cabs2(r1) + cabs2(r2));
       } else {  // EPI_CGR: r -= a Ap and ||r||^2 (CG.cu:71-76); Ap is never stored
         cplx<R> r1 = va[k], r2 = vb2[k];
-        r1.x -= are * o1.x - aim * o1.y;
-        r1.y -= are * o1.y + aim * o1.x;
-        r2.x -= are * o2.x - aim * o2.y;
-        r2.y -= are * o2.y + aim * o2.x;
+        if constexpr (sizeof(R) == 4) {  // real step size: packed pairs
+          r1 = pfma(o1, -are, r1);
+          r2 = pfma(o2, -are, r2);
+        } else {
+          r1.x -= are * o1.x - aim * o1.y;
+          r1.y -= are * o1.y + aim * o1.x;
+          r2.x -= are * o2.x - aim * o2.y;
+          r2.y -= are * o2.y + aim * o2.x;
+        }
         a.r[vb + i] = r1;
         a.r[vb + Nd + i] = r2;
         acc[0] += (double)(cabs2(r1) + cabs2(r2));
       }
     }
   }
-  cl.sync();  // remote shared memory must outlive the readers
+  // This CTA is done reading the other CTAs' planes.  A relaxed arrival (no wait for
+  // this CTA's global stores to drain); the matching wait below keeps every plane alive
+  // until all three CTAs have read it.
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
   if constexpr (EPI == EPI_CGR) {
     __shared__ double sred[32];
@@ -770,6 +806,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     }
     if constexpr (EPI == EPI_RESID) plane_fwd_decide<EPI>(a);
   }
+  asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");  // every CTA has read this plane
 }
 
 }  // namespace fame

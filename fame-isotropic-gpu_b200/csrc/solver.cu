@@ -83,6 +83,7 @@ struct fame_ctx {
   template <typename R> int plane_nt() const { return sizeof(R) == 4 ? plane_threads32 : plane_threads; }
   int pipe_ctas64 = 0;  // resident k_pencil_pipe<double> CTAs on the device
   int prefetch = 0;     // L2 prefetch one wave ahead in the CG stage kernels (fame_set_option; measured slower)
+  int self_prefetch = 1;  // CG plane stages: L2 prefetch of the CTA's own operands at its start
   int radix_order = 0;  // kRadixOrders index of the runtime-geometry axis plans
   int threads32_opt = 0, threads64_opt = 0;  // plane CTA sizes set by fame_set_option (0: rule)
   std::map<const void*, int> waves;  // resident CTAs of a stage kernel on the device
@@ -234,6 +235,7 @@ struct Ops {
                               : k_plane_inv<R, true, IN, PR, 0, DynGeom>;
       allow_smem(k, sm);
       a.pf_dist = IN == IN_CG && c->prefetch ? wave_ctas(c, k, c->template plane_nt<R>(), sm, 3) : 0;
+      a.self_pf = c->self_prefetch;
       P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_inv<R, false, IN, PR, 2, DynGeom>
@@ -247,6 +249,7 @@ struct Ops {
         }
       allow_smem(k, sm);
       a.pf_dist = IN == IN_CG && c->prefetch ? wave_ctas(c, k, nt, sm, 3) : 0;
+      a.self_pf = c->self_prefetch;
       P.launch(k, grid, dim3(nt), sm, a);
     }
   }
@@ -337,6 +340,7 @@ struct Ops {
                               : k_plane_fwd<R, true, EPI, PR, 0, DynGeom>;
       allow_smem(k, sm);
       a.pf_dist = EPI == EPI_CGR && c->prefetch ? wave_ctas(c, k, c->template plane_nt<R>(), sm, 3) : 0;
+      a.self_pf = c->self_prefetch;
       P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_fwd<R, false, EPI, PR, 2, DynGeom>
@@ -350,6 +354,7 @@ struct Ops {
         }
       allow_smem(k, sm);
       a.pf_dist = EPI == EPI_CGR && c->prefetch ? wave_ctas(c, k, nt, sm, 3) : 0;
+      a.self_pf = c->self_prefetch;
       P.launch(k, grid, dim3(nt), sm, a);
     }
   }
@@ -1241,6 +1246,8 @@ int fame_set_option(fame_ctx* c, const char* name, int value) {
   const bool threads_ok = value == 0 || (value >= 64 && value <= kPlaneThreads && value % 32 == 0);
   if (n == "prefetch" && (value == 0 || value == 1)) {
     c->prefetch = value;
+  } else if (n == "self_prefetch" && (value == 0 || value == 1)) {
+    c->self_prefetch = value;
   } else if (n == "radix_order" && value >= 0 && value < kNumRadixOrders) {
     Geom g;
     std::string err;
@@ -1275,6 +1282,8 @@ int fame_get_option(fame_ctx* c, const char* name, int* value) {
   const std::string n(name);
   if (n == "prefetch") {
     *value = c->prefetch;
+  } else if (n == "self_prefetch") {
+    *value = c->self_prefetch;
   } else if (n == "radix_order") {
     *value = c->radix_order;
   } else if (n == "plane_threads32") {

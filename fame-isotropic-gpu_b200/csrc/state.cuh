@@ -128,6 +128,7 @@ struct PlaneInArgs {
   Cond reset;             // loop condition cleared by this kernel when it starts a loop body
   int pf_dist;            // > 0: each CTA prefetches into L2 the operands of the CTA this
                           // many places later in launch order (about one wave ahead)
+  int self_pf;            // IN_CG: L2 prefetch of this CTA's own r, p and x at its start
 };
 
 template <typename R>
@@ -172,6 +173,7 @@ struct PlaneOutArgs {
   int nslots;
   double tol2;             // EPI_RESID: absolute tolerance^2 on ||b - A y||
   int pf_dist;             // > 0: L2 prefetch of the operands of the CTA this many places later
+  int self_pf;             // EPI_CGR: L2 prefetch of this CTA's own residual at its start
 };
 
 }  // namespace fame
