@@ -124,6 +124,59 @@ __device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"(n) : "memory");
 }
 
+// Shared-memory exchange between the CTAs of a cluster with an mbarrier (sm_90+).
+// A CTA initialises its barrier, announces the bytes it expects, and waits for them;
+// the other CTAs write into its shared memory with st.async, whose completion is
+// counted on that barrier.  Unlike a cluster barrier with release semantics, nothing
+// waits for the writers' outstanding global stores.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+// the address of this CTA's shared-memory location `local` in the CTA of cluster rank `rank`
+__device__ __forceinline__ unsigned mapa_u32(unsigned local, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+// makes an initialised barrier visible to the cluster's other CTAs (before a cluster barrier)
+__device__ __forceinline__ void mbar_init_fence_cluster() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(bar),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of the barrier for at most `max_cycles` SM clock cycles;
+// false if it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, long long max_cycles) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > max_cycles) return false;
+  return true;
+}
+// one complex value into cluster shared memory, counted on the destination's barrier
+__device__ __forceinline__ void st_async(unsigned addr, float2 v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];\n" ::"r"(addr),
+               "f"(v.x), "f"(v.y), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(unsigned addr, double2 v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];\n" ::"r"(addr),
+               "d"(v.x), "d"(v.y), "r"(bar)
+               : "memory");
+}
+
 // Kernels launched on the device, counted by each kernel's first thread.  Every
 // translation unit has its own counter; FAME_DEFINE_LAUNCH_GETTER exposes it.
 static __device__ unsigned long long g_launches;

@@ -46,7 +46,7 @@ struct DynGeom {
 // elements a thread stages per round in the static passes: plane passes (FP32 at
 // most 80 registers, two CTAs per SM) and pencil passes
 template <typename R> struct SEmax;
-template <> struct SEmax<float> { static constexpr int v = 12; };
+template <> struct SEmax<float> { static constexpr int v = 24; };
 template <> struct SEmax<double> { static constexpr int v = 12; };
 template <typename R> struct SPenEmax;
 template <> struct SPenEmax<float> { static constexpr int v = 24; };

@@ -114,6 +114,20 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       }
     }
   }
+  // Static geometries exchange the mixed components with st.async into the owner's
+  // plane, counted on the owner's barrier `xbar` (P values arrive per plane); the
+  // others use a cluster barrier after the exchange.
+  constexpr bool kAsyncMix = GP::kStatic;
+  __shared__ __align__(8) unsigned long long xbar;
+  const unsigned bar = smem_u32(&xbar);
+  // after a failed exchange (the fault marker), later launches skip their work: the
+  // cluster's rank-0 CTA reads the marker and all three CTAs act on its value
+  __shared__ int skip;
+  if (kAsyncMix && threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence_cluster();
+    skip = a.fault ? *(volatile int*)a.fault : 0;
+  }
   const double2* tab = a.tabs + (size_t)slot * g.tab_stride;
   for (int i = threadIdx.x; i < Lf; i += GP::plane_threads()) {
     twf[i] = a.tw[g.twf + i];
@@ -124,7 +138,20 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     if constexpr (!GEN) ly[i] = cvt<R>(tab[g.oLy + i]);
   }
   const cplx<R> lz = GEN ? mk<R>(0, 0) : cvt<R>(tab[g.oLz + s]);
-  cl.sync();  // every CTA of the cluster is running (and the tables are in place)
+  cl.sync();  // every CTA of the cluster is running (and the tables and barriers are in place)
+  if constexpr (kAsyncMix) {
+    if (*cl.map_shared_rank(&skip, 0)) {
+      cl.sync();  // rank 0's marker stays readable until all three have read it
+      return;
+    }
+  }
+  if (kAsyncMix && threadIdx.x == 0) mbar_arrive_expect_tx(bar, (unsigned)(P * sizeof(cplx<R>)));
+  unsigned rplane[3], rbar[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    rplane[c] = kAsyncMix ? mapa_u32(smem_u32(plane), c) : 0u;
+    rbar[c] = kAsyncMix ? mapa_u32(bar, c) : 0u;
+  }
 
   const long vb = (long)(slot * a.vec_per_slot + vec) * a.vstride;
   const int Nd = sl.Nd, off = sl.off;
@@ -254,11 +281,25 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
 #pragma unroll
         for (int c = 0; c < 3; c++) v[c] = cadd(cmul(Pc[c], x1), cmul(Pc[3 + c], x2));
       }
+      if constexpr (kAsyncMix) {
+        const unsigned o = (unsigned)((m * S + f) * sizeof(cplx<R>));
 #pragma unroll
-      for (int c = 0; c < 3; c++) dst[c][m * S + f] = v[c];
+        for (int c = 0; c < 3; c++) st_async(rplane[c] + o, v[c], rbar[c]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; c++) dst[c][m * S + f] = v[c];
+      }
     }
   }
-  cl.sync();
+  if constexpr (kAsyncMix) {
+    // this CTA's plane is complete once all P values have arrived.  A wait that runs out
+    // (about 0.1 s; it cannot unless the exchange is broken) records the fault and goes
+    // on, and later launches return at once (below), so the solve ends with an error.
+    if (!mbar_wait(bar, 0, 200000000LL) && a.fault) atomicExch(a.fault, 1);
+    __syncthreads();
+  } else {
+    cl.sync();
+  }
 
   // inverse 2-D transform of this component's plane (unnormalised): fast axis,
   // then mid axis.  One FFT call site per axis loop keeps the kernel within its

@@ -179,6 +179,11 @@ template <typename K> static int resident_ctas(K* k, size_t smem) {
   return std::max(1, per) * sms;
 }
 
+// Device ints of the context (c->flags): the condition flag of loop i at flags[i], its
+// trip counter and overflow marker at flags[kTrips + 2i], and a kernel fault marker
+// (a bounded wait that ran out) at flags[kFaultFlag].
+constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopRestart = 4, kFaultFlag = 30, kTrips = 32;
+
 struct Ops {
   fame_ctx* c;
   Program& P;
@@ -227,6 +232,7 @@ struct Ops {
     a.p32 = p32;
     a.sigma = sigma;
     a.T = T;
+    a.fault = c->flags.p ? c->flags.p + kFaultFlag : nullptr;
     const size_t sm = plane_smem<R>(g());
     dim3 grid(3 * g().Ls, nvec, nslots);
     if (g().general) {
@@ -601,9 +607,6 @@ static std::string cfg_key(const SolveCfg& s, bool graph) {
 
 // invAr (FAME_Main/FAME_Matrix_Vector_Production_Isotropic_invAr.cu:8-48) for the
 // Lanczos vector u_j of every live slot, leaving w in U[:, j+1]; then one Lanczos step.
-// device ints of the loop conditions: flag of loop i at flags[i], its trip counter
-// and overflow marker at flags[kTrips + 2i]
-constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopRestart = 4, kTrips = 32;
 static Cond loop_cond(Program& P, int* flags, int id, int cap, int loop_cap = 0) {
   return P.make_cond(flags + id, flags + kTrips + 2 * id, loop_cap > 0 ? std::min(cap, loop_cap) : cap);
 }
@@ -1012,6 +1015,10 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
           set_err("a device loop reached its trip cap (loop " + std::to_string(id) + ")");
           return FAME_ERR_WATCHDOG;
         }
+      if (hflags[kFaultFlag]) {
+        set_err("a bounded device wait ran out (shared-memory exchange of a plane cluster)");
+        return FAME_ERR_WATCHDOG;
+      }
       for (int q = 0; q < nb; q++) {
         const int kk = b0 + q;
         const bool gamma = hs[q].Nd == N - 1;

@@ -129,6 +129,7 @@ struct PlaneInArgs {
   int pf_dist;            // > 0: each CTA prefetches into L2 the operands of the CTA this
                           // many places later in launch order (about one wave ahead)
   int self_pf;            // IN_CG: L2 prefetch of this CTA's own r, p and x at its start
+  int* fault;             // set to 1 if a bounded wait of the component exchange ran out (or NULL)
 };
 
 template <typename R>
