@@ -479,23 +479,13 @@ __global__ void __launch_bounds__(kPencilThreads, GP::kStatic ? (sizeof(R) == 4 
   if constexpr (MODE == PEN_QBQ_CG) {
     // <p, Ap> for A = Q_r^* B^-1 Q_r: Q_r^* is N times the adjoint of Q_r (unnormalised
     // forward DFT against the 1/N-scaled inverse), so <p, Ap> = N ||B^-1/2 Q_r p||^2 =
-    // (1/N) sum_e |IDFT(Pi p)_e|^2 / eps_e.  It is real and positive: the CG step is
-    // a = ||r||^2 / <p, Ap> (CG.cu:57-63, with Zdotc(p, Ap) formed in the field domain).
+    // (1/N) sum_e |IDFT(Pi p)_e|^2 / eps_e, real and positive (CG.cu:57-63, with
+    // Zdotc(p, Ap) formed in the field domain).  This CTA writes its partial sum; the
+    // forward plane stage sums the slot's partials in order and forms a = ||r||^2 / <p, Ap>.
     double acc[1] = {(double)dot};
     __shared__ double sred[32];
     block_reduce<1>(acc, sred);
-    const int nblk = gridDim.x * gridDim.y;  // CTAs of this slot (vec_per_slot == 1 in solves)
-    double tot[1];
-    if (slot_reduce<1>(acc, a.partials + (size_t)slot * nblk, a.counters + slot, blockIdx.y * gridDim.x + blockIdx.x,
-                       nblk, tot)) {
-      if (threadIdx.x == 0) {
-        CgState* st = a.cg + slot;
-        const double pAp = tot[0] / g.N;
-        st->a_re = pAp > 0 ? st->r1 / pAp : 0.0;
-        st->a_im = 0.0;
-        __threadfence();
-      }
-    }
+    if (threadIdx.x == 0) a.partials[(size_t)slot * a.pstride + blockIdx.y * gridDim.x + blockIdx.x] = acc[0];
   }
 }
 
@@ -640,7 +630,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   if constexpr (EPI == EPI_CG || EPI == EPI_CGR) live = live && a.cg[slot].active;
   if constexpr (EPI == EPI_RESID) live = live && a.cg[slot].outer_active;
   if (!live) {
-    if constexpr (EPI == EPI_RESID || EPI == EPI_CGR) plane_fwd_decide<EPI>(a);
+    if constexpr (EPI == EPI_RESID) plane_fwd_decide<EPI>(a);
     return;
   }
   if constexpr (EPI == EPI_CGR) {
@@ -686,6 +676,16 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     const int m = e / Lf;
     cp_async_elem(plane + e + m * (S - Lf), T + e);
   }
+  __shared__ R s_step;
+  if constexpr (EPI == EPI_CGR) {
+    // the CG step a = ||r||^2 / <p, Ap> from the pencil stage's partial sums of this
+    // k-point, summed in order by one warp while the plane streams in (k_cg_decide forms
+    // the same sum for the solution update and the CG state)
+    if (threadIdx.x < 32) {
+      const double pAp = warp_sum_partials(a.partials + (size_t)slot * a.pstride, a.pen_parts) / g.N;
+      if (threadIdx.x == 0) s_step = (R)(pAp > 0 ? a.cg[slot].r1 / pAp : 0.0);
+    }
+  }
   cp_async_wait_all();
   __syncthreads();
   // forward 2-D transform.  General lattices (T*, FAME_FFT_CUDA.cu:128-150):
@@ -723,10 +723,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   constexpr int KB = GP::kStatic ? 4 : 2;
   const int NT = GP::plane_threads();
   R are = 0, aim = 0;
-  if constexpr (EPI == EPI_CGR) {
-    are = (R)a.cg[slot].a_re;
-    aim = (R)a.cg[slot].a_im;
-  }
+  if constexpr (EPI == EPI_CGR) are = s_step;  // real: <p, Ap> > 0
   for (int eb = e0 + threadIdx.x; eb < e1; eb += KB * NT) {
     cplx<R> t[KB][3], va[KB], vb2[KB];
 #pragma unroll
@@ -801,25 +798,11 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
   if constexpr (EPI == EPI_CGR) {
+    // this CTA's part of ||r||^2; k_cg_decide sums the slot's parts in order
     __shared__ double sred[32];
     double acc1[1] = {acc[0]};
     block_reduce<1>(acc1, sred);
-    const int nblk = gridDim.x;  // CTAs of this slot (vec_per_slot == 1 in solves)
-    double tot[1];
-    if (slot_reduce<1>(acc1, a.partials + (size_t)slot * nblk, a.counters + slot, blockIdx.x, nblk, tot)) {
-      if (threadIdx.x == 0) {
-        // r0 = r1, r1 = <r, r>, k++ and the loop test r1 > tol^2 && k <= maxit (CG.cu:37, :73-77)
-        CgState* st = a.cg + slot;
-        st->r0 = st->r1;
-        st->r1 = tot[0];
-        st->beta = st->r1 / st->r0;
-        st->iter++;
-        st->total++;
-        st->active = (st->r1 > st->tol2) && (st->iter <= st->maxit);
-        __threadfence();
-      }
-    }
-    plane_fwd_decide<EPI>(a);
+    if (threadIdx.x == 0) a.partials[(size_t)slot * a.pstride + a.pen_parts + blockIdx.x] = acc1[0];
   }
   if constexpr (EPI == EPI_CG || EPI == EPI_RESID) {
     __shared__ double sred[2 * 32];

@@ -104,6 +104,7 @@ struct fame_ctx {
   const float* ibq32() const { return g.general ? invB32q.p : invB32.p; }
   // per-batch workspace
   int cap_slots = 0, cap_nstep = 0, cap_nwant = 0;
+  long part_stride = 0;  // doubles of `partials` per slot
   bool cap_mixed = false, cap_vec = false;
   DBuf<Slot> slots;
   DBuf<double2> tabs;
@@ -207,6 +208,27 @@ struct Ops {
 
   template <typename R> const cplx<R>* tw() const;
 
+  // partial sums per slot of the fused FP32 CG kernels: the pencil stage's <p, Ap>
+  // (one per CTA of a slot), then the forward plane stage's ||r||^2
+  int cg_pen_parts() const { return 3 * g().Lm * ((g().Lf + pencil_tw<float>() - 1) / pencil_tw<float>()); }
+  int cg_fwd_parts() const { return 3 * g().Ls; }
+
+  // end of a fused FP32 CG iteration: step size, r1, beta, counters, loop decision
+  void cg_decide(Cond cond) {
+    CgDecideArgs d;
+    d.slots = c->slots.p;
+    d.cg = c->cg.p;
+    d.partials = c->partials.p;
+    d.pstride = c->part_stride;
+    d.pen_parts = cg_pen_parts();
+    d.fwd_parts = cg_fwd_parts();
+    d.N = g().N;
+    d.counters = c->counters.p;
+    d.cond = cond;
+    d.nslots = nslots;
+    P.launch(k_cg_decide, dim3(nslots), dim3(32), 0, d);
+  }
+
   // plane inverse stage
   template <typename R, int IN, bool PR>
   void plane_inv(const cplx<R>* in, cplx<R>* T, int nvec, long vstride, long fstride, int sigma,
@@ -279,6 +301,7 @@ struct Ops {
     a.gate = gate;
     a.partials = c->partials.p;
     a.counters = c->counters.p;
+    a.pstride = c->part_stride;
     a.TW = pencil_tw<R>();
     a.nslots = nslots;
     const size_t sm = pencil_smem<R>(g());
@@ -338,6 +361,8 @@ struct Ops {
     a.cond = cond;
     a.nslots = nslots;
     a.tol2 = tol2;
+    a.pstride = c->part_stride;
+    a.pen_parts = cg_pen_parts();
     const size_t sm = plane_smem<R>(g());
     dim3 grid(3 * g().Ls, nvec, nslots);
     if (g().general) {
@@ -412,8 +437,10 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
   c->cg.ensure(nslots);
   c->lz.ensure(nslots);
   const size_t lzblk = (M + kLzRows - 1) / kLzRows;
-  const size_t part = std::max({lzblk * (2 * 64 + 1), (size_t)3 * g.Ls * 2 * 16, (size_t)1184 * 4});
+  const size_t part = std::max({lzblk * (2 * 64 + 1), (size_t)3 * g.Ls * 2 * 16, (size_t)1184 * 4,
+                                 (size_t)3 * g.Lm * g.Lf + 3 * g.Ls});
   c->partials.ensure((size_t)nslots * part);
+  c->part_stride = (long)part;
   c->counters.ensure(nslots + 1);
   FAME_CK(cudaMemset(c->counters.p, 0, (nslots + 1) * sizeof(unsigned)));
   c->tri_ctr.ensure(1);
@@ -641,14 +668,16 @@ static void emit_step(Ops& o, const SolveCfg& s, LzArgs L, int j, int* flag_base
     P.while_loop(outer, [&] {
       P.launch(k_cg32_init, dim3(nvb, 1, s.nslots), dim3(256), 0, o.va(inner), (const double2*)c->r64.p,
                c->r32.p, c->x32.p, s.inner_tol * s.inner_tol, s.inner_maxit, tol2, outer);
-      // FP32 CG, three kernels per iteration: p and the deferred x update with the
-      // 2 -> 3 mix; the slow-axis transforms with <p, Ap>; the 3 -> 2 unmix with
-      // r -= a Ap, ||r||^2 and the loop decision (Ap is never stored)
+      // FP32 CG per iteration: p and the deferred x update with the 2 -> 3 mix; the
+      // slow-axis transforms with the partial sums of <p, Ap>; the 3 -> 2 unmix with
+      // r -= a Ap and the partial sums of ||r||^2 (Ap is never stored); a one-warp-per-slot
+      // kernel that ends the iteration (step size, beta, loop decision)
       P.while_loop(inner, [&] {
         o.plane_inv<float, IN_CG, false>(nullptr, c->T32.p, 1, M, F, 0, c->p32.p, c->r32.p, nullptr, nullptr,
                                          inner, c->x32.p);
         o.pencil<float, PEN_QBQ_CG>(c->T32.p, 1, F, c->ibq32(), 1);
         o.plane_fwd<float, EPI_CGR, false>(c->T32.p, nullptr, 1, M, F, nullptr, nullptr, inner, 0.0, c->r32.p);
+        o.cg_decide(inner);
       });
       o.plane_inv<double, IN_REFINE, false>(nullptr, c->T64.p, 1, M, F, 0, nullptr, nullptr, c->x64.p,
                                             c->x32.p, Cond{}, nullptr, c->p32.p);
@@ -1480,6 +1509,7 @@ int fame_bench_cg(fame_ctx* c, const double* k, int reps, int nbatch, double* ms
       o.pencil<float, PEN_QBQ_CG>(c->T32.p, 1, F, c->ibq32(), 1);
       FAME_CK(cudaEventRecord(ev[2], c->stream));
       o.plane_fwd<float, EPI_CGR, false>(c->T32.p, nullptr, 1, M, F, nullptr, nullptr, Cond{}, 0.0, c->r32.p);
+      o.cg_decide(Cond{});
       FAME_CK(cudaEventRecord(ev[3], c->stream));
       FAME_CK(cudaEventSynchronize(ev[3]));
       if (it == 0) continue;  // warm-up (the p = r iteration)

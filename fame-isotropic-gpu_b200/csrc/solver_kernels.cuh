@@ -120,6 +120,52 @@ __global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* r, const
   }
 }
 
+// ---------------------------------------------------------------- fused FP32 CG: end of an iteration
+// One CTA per slot.  From the partial sums the iteration's kernels wrote (the pencil
+// stage's <p, Ap> parts, then the forward plane stage's ||r||^2 parts): the step size
+// a = r1 / <p, Ap> (the same ordered sum as the forward plane stage formed), r0 = r1,
+// r1 = ||r||^2, beta = r1 / r0, k++ and the loop test r1 > tol^2 && k <= maxit
+// (CG.cu:37, :57-77); the last CTA of the grid sets the WHILE condition.
+struct CgDecideArgs {
+  const Slot* slots;
+  CgState* cg;
+  const double* partials;
+  long pstride;
+  int pen_parts, fwd_parts;
+  int N;
+  unsigned* counters;  // [nslots] unused here, [nslots] = grid ticket
+  Cond cond;
+  int nslots;
+};
+
+__global__ void __launch_bounds__(32) k_cg_decide(CgDecideArgs d) {
+  FAME_COUNT_LAUNCH();
+  const int slot = blockIdx.x;
+  CgState* st = d.cg + slot;
+  if (d.slots[slot].active && st->active) {
+    const double* p = d.partials + (size_t)slot * d.pstride;
+    const double pAp = warp_sum_partials(p, d.pen_parts) / d.N;
+    const double rr = warp_sum_partials(p + d.pen_parts, d.fwd_parts);
+    if (threadIdx.x == 0) {
+      st->a_re = pAp > 0 ? st->r1 / pAp : 0.0;
+      st->a_im = 0.0;
+      st->r0 = st->r1;
+      st->r1 = rr;
+      st->beta = st->r1 / st->r0;
+      st->iter++;
+      st->total++;
+      st->active = (st->r1 > st->tol2) && (st->iter <= st->maxit);
+    }
+  }
+  if (grid_last(d.counters + d.nslots, gridDim.x)) {
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int q = 0; q < d.nslots; q++) any |= d.slots[q].active && d.cg[q].active;
+      decide_cond(d.cond, any);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- invAr prologue
 // rhs = u / sqrt(Lambda_q) (…invAr.cu:26), CG start x = 0, r = rhs (CG.cu:30-33).
 // Plain FP64 (MIXED = false): r, x are the FP64 CG vectors.  Mixed: b = rhs, y = 0,

@@ -147,8 +147,9 @@ struct PencilArgs {
   const cplx<R>* in;       // PEN_QRS_IN: spatial field in
   CgState* cg;             // optional activity gate; PEN_QBQ_CG writes the step size a
   int gate;                // 0 none, 1 CG active, 2 outer refinement active
-  double* partials;        // PEN_QBQ_CG: [nslots][CTAs per slot] partial sums
-  unsigned* counters;      // PEN_QBQ_CG: [nslots] ticket counters
+  double* partials;        // PEN_QBQ_CG: partial sums of <p, Ap>, [slot * pstride + CTA of the slot]
+  unsigned* counters;      // (unused by PEN_QBQ_CG)
+  long pstride;            // per-slot stride of `partials`
   int TW;                  // fast positions per CTA
   int nslots;              // k-points of the launch (k_pencil_pipe walks all their tiles)
   int pf_dist;             // > 0: L2 prefetch of the tile of the CTA this many places later
@@ -175,6 +176,32 @@ struct PlaneOutArgs {
   double tol2;             // EPI_RESID: absolute tolerance^2 on ||b - A y||
   int pf_dist;             // > 0: L2 prefetch of the operands of the CTA this many places later
   int self_pf;             // EPI_CGR: L2 prefetch of this CTA's own residual at its start
+  long pstride;            // EPI_CGR: per-slot stride of `partials`
+  int pen_parts;           // EPI_CGR: the pencil's <p, Ap> partials per slot (at the slot's start);
+                           // this kernel's ||r||^2 partials follow them
 };
+
+// Ordered sum of n partial sums by one warp (lane-strided, then a fixed shuffle tree):
+// every caller gets the same bits, so kernels that need the same CG scalar (the step
+// size) agree exactly.  Valid in all lanes.
+__device__ __forceinline__ double warp_sum_partials(const double* p, int n) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  // 16 independent loads per lane in flight per round (a few hundred partials take
+  // one or two L2 round trips, not one per element)
+  for (int b = 0; b < n; b += 32 * 16) {
+    double v[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int i = b + u * 32 + lane;
+      v[u] = i < n ? p[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; u++) s += v[u];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
 
 }  // namespace fame
