@@ -121,6 +121,8 @@ struct fame_ctx {
   int dev_vec_nk = 0, dev_vec_nwant = 0;
   std::vector<int> dev_vec_gamma;
   DBuf<double> adj;  // fame_adjoint_vjp: [nwant] w, [nwant] grad_w, [nwant] denominators
+  DBuf<double> bpart;     // per-band partial sums of the solve's split reductions (kBandSplit per band)
+  DBuf<double> adj_part;  // the same for the adjoint entry points (never read by a recorded solve)
   DBuf<int> eps_bad;  // fame_set_eps_device: [0] bad count, [1] first bad edge
   // recorded programs keyed by configuration
   std::map<std::string, std::unique_ptr<Program>> progs;
@@ -183,6 +185,8 @@ template <typename K> static int resident_ctas(K* k, size_t smem) {
 // Device ints of the context (c->flags): the condition flag of loop i at flags[i], its
 // trip counter and overflow marker at flags[kTrips + 2i], and a kernel fault marker
 // (a bounded wait that ran out) at flags[kFaultFlag].
+// CTAs per band of the split per-band reductions (band statistics, norms, adjoint)
+constexpr int kBandSplit = 64;
 constexpr int kLoopCG = 0, kLoopOuter = 1, kLoopInner = 2, kLoopRestart = 4, kFaultFlag = 30, kTrips = 32;
 
 struct Ops {
@@ -476,6 +480,7 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
   c->p64.ensure((size_t)nslots * M);
   c->Ap64.ensure((size_t)nslots * M);
   if (vec) c->E.ensure((size_t)nslots * nwant * 3 * N);
+  c->bpart.ensure((size_t)nslots * nwant * kBandSplit * 4);
   c->cap_slots = nslots;
   c->cap_nstep = nstep;
   c->cap_nwant = nwant;
@@ -484,11 +489,30 @@ static void ensure_workspace(fame_ctx* c, int nslots, int nstep, int nwant, bool
 }
 
 // ------------------------------------------------------------------ statistics kernels
-// Per (slot, band): y = Ritz vector, v = QBQ(Sigma y).  Reduces
-// ||Sigma (Sigma v - lambda y)||^2, ||Sigma y||^2, Re<Sigma y, v>, ||y||^2.
+// Per-band sums over a reduced or field vector split over kBandSplit CTAs per band: each CTA
+// writes its partial sums, and one warp per band adds them in a fixed order
+// (k_rows_sum), so the sums are deterministic and every band's work spreads over the SMs.
+
+// [nrows][nsplit][nq] partials -> [nrows][nq] sums, one warp per row (blockIdx.x band,
+// blockIdx.y slot; row = slot * nband + band).  slots == nullptr: every row is live.
+__global__ void __launch_bounds__(32) k_rows_sum(const Slot* slots, int nband, const double* part, int nsplit,
+                                                 int nq, double* out) {
+  FAME_COUNT_LAUNCH();
+  const int band = blockIdx.x, slot = blockIdx.y;
+  if (slots && !slots[slot].active) return;
+  const size_t row = (size_t)slot * nband + band;
+  for (int q = 0; q < nq; q++) {
+    const double v = warp_sum_strided(part + row * nsplit * nq + q, nsplit, nq);
+    if (threadIdx.x == 0) out[row * nq + q] = v;
+  }
+}
+
+// Per (slot, band): y = Ritz vector, v = QBQ(Sigma y).  Partial sums of
+// ||Sigma (Sigma v - lambda y)||^2, ||Sigma y||^2, Re<Sigma y, v>, ||y||^2 over this
+// CTA's chunk of the 2 Nd entries (k_rows_sum adds them).
 __global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* EV, const double2* AV,
                                                     long vstride, int nwant, const double* theta,
-                                                    int nstep, double* stats) {
+                                                    int nstep, double* part) {
   FAME_COUNT_LAUNCH();
   const int band = blockIdx.y, slot = blockIdx.z;
   const Slot sl = va.slots[slot];
@@ -497,8 +521,10 @@ __global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* E
   const double2* tab = va.tabs + (size_t)slot * va.g.tab_stride;
   const long base = (long)(slot * nwant + band) * vstride;
   const int n = 2 * sl.Nd;
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
   double acc[4] = {0, 0, 0, 0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     const double s = lq_sqrt_at(va.g, tab, full_index(i, sl.Nd, sl.off));
     const double2 y = EV[base + i], v = AV[base + i];
     const double rx = s * (s * v.x - lam * y.x), ry = s * (s * v.y - lam * y.y);
@@ -510,29 +536,47 @@ __global__ void __launch_bounds__(256) k_band_stats(VecArgs va, const double2* E
   __shared__ double sred[4 * 32];
   block_reduce<4>(acc, sred);
   if (threadIdx.x == 0)
-    for (int q = 0; q < 4; q++) stats[((size_t)slot * nwant + band) * 4 + q] = acc[q];
+    for (int q = 0; q < 4; q++) part[(((size_t)slot * nwant + band) * gridDim.x + blockIdx.x) * 4 + q] = acc[q];
 }
 
-// ||E||^2 per (slot, band) and the reference's scaling E *= ||E||
-// (FAME_Fast_Algorithms_Isotropic.cu:119-121).
-__global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, double2* E, long fstride,
-                                                          int nwant, long n3, double* norms) {
+// Partial sums of ||E||^2 per (slot, band) over this CTA's chunk of the 3N entries.
+__global__ void __launch_bounds__(256) k_band_norm_part(const Slot* slots, const double2* E, long fstride,
+                                                        int nwant, long n3, double* part) {
   FAME_COUNT_LAUNCH();
-  const int band = blockIdx.x, slot = blockIdx.y;
+  const int band = blockIdx.y, slot = blockIdx.z;
   if (!slots[slot].active) return;
-  double2* e = E + (long)(slot * nwant + band) * fstride;
+  const double2* e = E + (long)(slot * nwant + band) * fstride;
+  const long chunk = (n3 + gridDim.x - 1) / gridDim.x;
+  const long i0 = blockIdx.x * chunk, i1 = min(n3, i0 + chunk);
   double acc[1] = {0.0};
-  for (long i = threadIdx.x; i < n3; i += blockDim.x) acc[0] += cabs2(e[i]);
+  for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) acc[0] += cabs2(e[i]);
   __shared__ double sred[32];
   block_reduce<1>(acc, sred);
+  if (threadIdx.x == 0) part[((size_t)slot * nwant + band) * gridDim.x + blockIdx.x] = acc[0];
+}
+
+// The reference's scaling E *= ||E|| (FAME_Fast_Algorithms_Isotropic.cu:119-121): every
+// CTA forms ||E|| from the nsplit partials in the same order, then scales its chunk.
+__global__ void __launch_bounds__(256) k_band_scale(const Slot* slots, double2* E, long fstride, int nwant,
+                                                    long n3, const double* part, int nsplit, double* norms) {
+  FAME_COUNT_LAUNCH();
+  const int band = blockIdx.y, slot = blockIdx.z;
+  if (!slots[slot].active) return;
+  const size_t row = (size_t)slot * nwant + band;
   __shared__ double nrm;
-  if (threadIdx.x == 0) {
-    nrm = sqrt(acc[0]);
-    norms[slot * nwant + band] = nrm;
+  if (threadIdx.x < 32) {
+    const double v = sqrt(warp_sum_strided(part + row * nsplit, nsplit, 1));
+    if (threadIdx.x == 0) {
+      nrm = v;
+      if (blockIdx.x == 0) norms[row] = v;
+    }
   }
   __syncthreads();
   const double s = nrm;
-  for (long i = threadIdx.x; i < n3; i += blockDim.x) e[i] = cscale(e[i], s);
+  double2* e = E + (long)row * fstride;
+  const long chunk = (n3 + gridDim.x - 1) / gridDim.x;
+  const long i0 = blockIdx.x * chunk, i1 = min(n3, i0 + chunk);
+  for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) e[i] = cscale(e[i], s);
 }
 
 // ------------------------------------------------------------------ adjoint
@@ -540,15 +584,19 @@ __global__ void __launch_bounds__(1024) k_band_norm_scale(const Slot* slots, dou
 // -w^2 |E_e|^2 / (E^H B E), so dw/dB_e = -(w/2) |E_e|^2 / (E^H B E).  With one
 // permittivity per voxel (B_x = B_y = B_z = eps) the voxel gradient sums its three
 // edges.  Bands with w = 0 (Gamma patch) get zero gradient.
-__global__ void __launch_bounds__(1024) k_adj_den(const double2* E, const double* B, long n3, double* den) {
+// Partial sums of E^H B E per band (blockIdx.y) over this CTA's chunk of the 3N edges;
+// k_rows_sum adds the gridDim.x partials of a band in order.
+__global__ void __launch_bounds__(256) k_adj_den(const double2* E, const double* B, long n3, double* part) {
   FAME_COUNT_LAUNCH();
-  const int band = blockIdx.x;
+  const int band = blockIdx.y;
   const double2* e = E + (long)band * n3;
+  const long chunk = (n3 + gridDim.x - 1) / gridDim.x;
+  const long i0 = blockIdx.x * chunk, i1 = min(n3, i0 + chunk);
   double acc[1] = {0.0};
-  for (long i = threadIdx.x; i < n3; i += blockDim.x) acc[0] += B[i] * cabs2(e[i]);
+  for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) acc[0] += B[i] * cabs2(e[i]);
   __shared__ double sred[32];
   block_reduce<1>(acc, sred);
-  if (threadIdx.x == 0) den[band] = acc[0];
+  if (threadIdx.x == 0) part[(size_t)band * gridDim.x + blockIdx.x] = acc[0];
 }
 
 __global__ void __launch_bounds__(256) k_adj_grad(const double2* E, const double* w, const double* den, long N,
@@ -752,16 +800,20 @@ static void record_solve(fame_ctx* c, Program& P, const SolveCfg& s) {
   o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
   o.pencil<double, PEN_QBQ>(c->Tb.p, s.nwant, F, c->ibq64(), 0);
   o.plane_fwd<double, EPI_OUT, false>(c->Tb.p, c->AV.p, s.nwant, M, F);
-  P.launch(k_band_stats, dim3(1, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{}),
+  P.launch(k_band_stats, dim3(kBandSplit, s.nwant, s.nslots), dim3(256), 0, o.va(Cond{}),
            (const double2*)c->EV.p, (const double2*)c->AV.p, M, s.nwant, (const double*)c->theta.p, s.nstep,
-           c->stats.p);
+           c->bpart.p);
+  P.launch(k_rows_sum, dim3(s.nwant, s.nslots), dim3(32), 0, (const Slot*)c->slots.p, s.nwant,
+           (const double*)c->bpart.p, kBandSplit, 4, c->stats.p);
   if (s.vec || s.enorm) {
     // E = B^{-1} Q_r (Sigma ev), scaled by its norm (FAME_Fast_Algorithms_Isotropic.cu:107-122);
     // the norms go after the band statistics
     o.plane_inv<double, IN_VEC, false>(c->EV.p, c->Tb.p, s.nwant, M, F, 1);
     o.pencil<double, PEN_QR_OUT>(c->Tb.p, s.nwant, F, c->invB64.p, 0, c->E.p);
-    P.launch(k_band_norm_scale, dim3(s.nwant, s.nslots), dim3(1024), 0, (const Slot*)c->slots.p, c->E.p, F,
-             s.nwant, F, c->stats.p + (size_t)s.nslots * s.nwant * 4);
+    P.launch(k_band_norm_part, dim3(kBandSplit, s.nwant, s.nslots), dim3(256), 0, (const Slot*)c->slots.p,
+             (const double2*)c->E.p, F, s.nwant, F, c->bpart.p);
+    P.launch(k_band_scale, dim3(4 * kBandSplit, s.nwant, s.nslots), dim3(256), 0, (const Slot*)c->slots.p, c->E.p, F,
+             s.nwant, F, (const double*)c->bpart.p, kBandSplit, c->stats.p + (size_t)s.nslots * s.nwant * 4);
   }
 }
 
@@ -852,7 +904,7 @@ void fame_ctx_destroy(fame_ctx* c) {
     b->release();
   for (auto* b : {&c->r32, &c->x32, &c->p32, &c->T32, &c->tw32}) b->release();
   for (auto* b : {&c->invB64, &c->invB64q, &c->B64, &c->partials, &c->T0, &c->T1, &c->hcoef, &c->theta, &c->Z, &c->G,
-                  &c->stats, &c->adj})
+                  &c->stats, &c->adj, &c->bpart, &c->adj_part})
     b->release();
   c->eps_bad.release();
   c->invB32.release();
@@ -1606,7 +1658,10 @@ int fame_adjoint_vjp(fame_ctx* c, int kidx, const double* freq, const double* gr
     }
     FAME_CK(cudaMemcpyAsync(c->adj.p, wg.data(), wg.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     if (nvec > 0) {
-      k_adj_den<<<nvec, 1024, 0, c->stream>>>(E, c->B64.p, 3 * N, c->adj.p + 2 * nwant);
+      c->adj_part.ensure((size_t)nvec * kBandSplit);
+      k_adj_den<<<dim3(kBandSplit, nvec), 256, 0, c->stream>>>(E, c->B64.p, 3 * N, c->adj_part.p);
+      FAME_CK(cudaGetLastError());
+      k_rows_sum<<<nvec, 32, 0, c->stream>>>(nullptr, nvec, c->adj_part.p, kBandSplit, 1, c->adj.p + 2 * nwant);
       FAME_CK(cudaGetLastError());
     }
     k_adj_vjp<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(E, c->adj.p, nwant, first, N, grad_dev);
@@ -1643,7 +1698,10 @@ int fame_adjoint(fame_ctx* c, const double* freq, const double* evec, int nwant,
     den.ensure(nwant);
     grad.ensure((size_t)nwant * N);
     FAME_CK(cudaMemcpyAsync(w.p, freq, nwant * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    k_adj_den<<<nwant, 1024, 0, c->stream>>>(E, c->B64.p, 3 * N, den.p);
+    c->adj_part.ensure((size_t)nwant * kBandSplit);
+    k_adj_den<<<dim3(kBandSplit, nwant), 256, 0, c->stream>>>(E, c->B64.p, 3 * N, c->adj_part.p);
+    FAME_CK(cudaGetLastError());
+    k_rows_sum<<<nwant, 32, 0, c->stream>>>(nullptr, nwant, c->adj_part.p, kBandSplit, 1, den.p);
     FAME_CK(cudaGetLastError());
     k_adj_grad<<<dim3((unsigned)((N + 255) / 256), nwant), 256, 0, c->stream>>>(E, w.p, den.p, N, grad.p);
     FAME_CK(cudaGetLastError());

@@ -74,7 +74,7 @@ struct VecArgs {
 
 // ---------------------------------------------------------------- CG update
 // x += a p ; r -= a Ap ; r1 = <r, r>  (FAME_Main/CG.cu:65-76); then beta, the
-// iteration counter and the loop test r1 > tol^2 && k <= maxit (:302).
+// iteration counter and the loop test r1 > tol^2 && k <= maxit (:37, :77).
 template <typename R>
 __global__ void __launch_bounds__(256) k_cg_update(VecArgs va, cplx<R>* r, const cplx<R>* Ap) {
   FAME_COUNT_LAUNCH();
@@ -435,10 +435,11 @@ __global__ void __launch_bounds__(256) k_lz_dots(VecArgs va, LzArgs L, int j) {
   __syncthreads();
   if (!last) return;
   __threadfence();
-  for (int v = threadIdx.x; v < nval; v += blockDim.x) {
-    double s = 0.0;
-    for (int q = 0; q < (int)gridDim.x; q++) s += *((volatile double*)&part[(size_t)q * (2 * 64 + 1) + v]);
-    red[v] = s;  // reuse (no other warps read red any more)
+  // one warp per value, lanes strided over the CTAs' partials (a fixed order)
+  __syncthreads();
+  for (int v = wid; v < nval; v += nw) {
+    const double s = warp_sum_strided_cg(part + v, gridDim.x, 2 * 64 + 1);
+    if (lane == 0) red[v] = s;  // reuse (every warp has read its own red entries)
   }
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -181,6 +181,27 @@ struct PlaneOutArgs {
                            // this kernel's ||r||^2 partials follow them
 };
 
+// Ordered sum of p[0], p[stride], ..., p[(n - 1) stride] by one warp (lane-strided,
+// then a fixed shuffle tree); valid in all lanes.
+__device__ __forceinline__ double warp_sum_strided(const double* p, int n, int stride) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += p[(size_t)i * stride];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// warp_sum_strided over data other CTAs of this grid wrote (loads through L2, not L1).
+__device__ __forceinline__ double warp_sum_strided_cg(const double* p, int n, int stride) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += __ldcg(p + (size_t)i * stride);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
 // Ordered sum of n partial sums by one warp (lane-strided, then a fixed shuffle tree):
 // every caller gets the same bits, so kernels that need the same CG scalar (the step
 // size) agree exactly.  Valid in all lanes.

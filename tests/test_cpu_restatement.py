@@ -33,6 +33,18 @@ def test_sc16_matches_reference_build():
         assert out["converged"][q] == 1
 
 
+def test_sc32_matches_reference_build():
+    """SC 32^3 (the 96^3 material), one k-point off Gamma, 8 bands."""
+    par = load_pre("sc32")
+    ref = load_ref("sc32")
+    kp = ref["kpoints"][1]
+    out = fc.solve(par, edge_eps(par), np.array([kp["wave_vec"]]), len(kp["freq"]), 40, 1e-10, 100, 1e-10, 1000)
+    rf = np.array(kp["freq"])
+    assert np.max(np.abs(out["freq"][0] - rf) / rf) < 1e-8
+    assert out["es_iter"][0] == kp["es_iter"]
+    assert out["converged"][0] == 1
+
+
 def test_block_timer_runs():
     par = load_pre("sc16")
     t_cg, t_lz = fc.time_blocks(par, edge_eps(par), par["kpoints"][1], iters=3, jstep=5)
