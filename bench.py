@@ -360,7 +360,7 @@ def run_ours(args):
             if tj.get("grid") == list(W["grid"]):
                 trc = int(nb * tj["dram_bytes_per_kpoint"])
         roof = {"bound": "hbm", "kernel": f"FP32 CG iteration = plane_inv<IN_CG> + pencil<PEN_QBQ_CG> + "
-                                          f"plane_fwd<EPI_CGR> over a batch of {nb} k-points",
+                                          f"plane_fwd<EPI_CGR> + cg_decide over a batch of {nb} k-points",
                 "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
                 "peak_source": src, "traffic": trc, "algorithmic_bytes": algc, "batch": nb,
                 "ms_per_launch": round(msc, 5), "us_per_kpoint": round(msc * 1e3 / nb, 2),
