@@ -113,12 +113,14 @@ def test_metric_grid_qbq_properties():
     assert rel(q32, x / eps) < 1e-5
 
 
-@pytest.mark.parametrize("grid", [(23, 19, 34), (34, 23, 19), (17, 38, 21)])
+@pytest.mark.parametrize("grid", [(23, 19, 34), (34, 23, 19), (17, 38, 21), (107, 6, 8), (92, 107, 4)])
 def test_prime_axis_lengths_match_oracle(grid):
     """Axis lengths with prime factors >= 17 (alone, and after a radix-2 or radix-3
     pass, so the prime pass runs with and without Stockham twiddles) in the plane
     and the pencil stages: a simple-cubic lattice with a random B, FP64 within 1e-12
-    and FP32 within 1e-5 of the oracle."""
+    and FP32 within 1e-5 of the oracle.  A whole-line prime axis runs in FP32 on the
+    tensor cores: 107 points along the fast axis (6 lines per plane) and along the mid
+    axis (92 lines per plane: two rounds of line tiles)."""
     N = int(np.prod(grid))
     par = dict(grid=grid, mesh_len=np.array([1.0 / g for g in grid]),
                lattice_vec_a=np.array([1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0]), simple=True,
