@@ -74,6 +74,8 @@ inline int layout_geom(const fame_lattice& L, Geom& g, long max_points, std::str
   g.hx = L.mesh_len[0];
   g.hy = L.mesh_len[1];
   g.hz = L.mesh_len[2];
+  g.ihz = 1.0 / g.hz;
+  g.tnz = 2.0 / g.Nz;
   g.Ls = g.general ? g.Nx : g.Nz;
   g.Lm = g.Ny;
   g.Lf = g.general ? g.Nz : g.Nx;

@@ -37,6 +37,8 @@ struct Geom {
   int Ls, Lm, Lf, P;  // slow / mid / fast lengths, plane size
   int S;              // row pitch of a plane in shared memory: Lf rounded up to odd
   double hx, hy, hz;
+  double ihz;  // 1 / hz
+  double tnz;  // 2 / Nz
   AxisPlan pf, pm, ps;
   // per-slot table offsets (in double2 units) inside a slot's table block
   int oLx, oLy, oLz, oDx, oDy, oDz, oExy, oWz, oDky, oPhi, oDkx;
@@ -64,7 +66,7 @@ __device__ __forceinline__ void lambdas_at(const Geom& g, const double2* tab, in
     Lx = tab[g.oLx + s];
     Ly = tab[g.oLy + s * g.Ny + m];
     const double2 e = cmul(tab[g.oExy + s * g.Ny + m], tab[g.oWz + f]);
-    Lz = make_double2((e.x - 1.0) / g.hz, e.y / g.hz);
+    Lz = make_double2((e.x - 1.0) * g.ihz, e.y * g.ihz);
   }
 }
 

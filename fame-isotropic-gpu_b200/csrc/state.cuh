@@ -90,11 +90,13 @@ __device__ __forceinline__ bool grid_last(unsigned* ctr, unsigned total) {
 template <typename R>
 __device__ __forceinline__ cplx<R> dkz_at(const Geom& g, const double2* tab, int x, int y, int z) {
   const double ph = tab[g.oPhi + x * g.Ny + y].x;
+  const double a = ph * z * g.tnz;  // e^{i pi a}, a = 2 ph z / Nz
   if constexpr (sizeof(R) == 8) {
-    // exact argument reduction of ph*z/Nz: the integer part of ph*z contributes 2*pi*n
-    return expipi(2.0 * ph * z / g.Nz);
+    return expipi(a);
   } else {
-    return to_f(expipi(2.0 * ph * z / g.Nz));
+    // FP32: the argument reduced to [-1, 1] in FP64 (a - 2n changes nothing), then a
+    // single-precision sincospi
+    return expipi((float)(a - 2.0 * rint(0.5 * a)));
   }
 }
 
