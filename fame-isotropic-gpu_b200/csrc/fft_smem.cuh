@@ -550,7 +550,7 @@ __device__ __forceinline__ bool prime_pass(cplx<R>* buf, int n, int r, int Ns, L
 }
 
 template <typename R> struct PrimeBlock;
-template <> struct PrimeBlock<float> { static constexpr int mu = 4, ml = 4; };
+template <> struct PrimeBlock<float> { static constexpr int mu = 4, ml = 3; };
 template <> struct PrimeBlock<double> { static constexpr int mu = 2, ml = 2; };
 
 // Passes for radix 7, 11, 13 (LEVEL >= 1) and primes >= 17 (LEVEL 2).

@@ -119,6 +119,11 @@ inline int layout_geom(const fame_lattice& L, Geom& g, long max_points, std::str
 inline int geom_level(const Geom& g) {
   return std::max(plan_level(g.pf), std::max(plan_level(g.pm), plan_level(g.ps)));
 }
+// ... the plane stages' axes (fast, mid) and the pencil stage's axis (slow) alone: each
+// stage kernel runs the lowest level its own axes need (fewer registers, no spills
+// from passes it never runs)
+inline int plane_level(const Geom& g) { return std::max(plan_level(g.pf), plan_level(g.pm)); }
+inline int pencil_level(const Geom& g) { return plan_level(g.ps); }
 
 // Threads of a runtime-geometry plane CTA: about 8 plane elements per thread, at most
 // 512; at most 256 when two planes of precision R fit one SM's shared memory (more,

@@ -87,7 +87,8 @@ struct fame_ctx {
   int radix_order = 0;  // kRadixOrders index of the runtime-geometry axis plans
   int threads32_opt = 0, threads64_opt = 0;  // plane CTA sizes set by fame_set_option (0: rule)
   std::map<const void*, int> waves;  // resident CTAs of a stage kernel on the device
-  int rare = 0;         // fft_lines level the axis plans need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
+  int rare = 0;      // fft_lines level the plane axes need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
+  int rare_pen = 0;  // the same for the pencil (slow) axis
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   int loop_cap = 0;     // fame_set_loop_cap: bound on every device loop's trips (0: defaults)
   bool have_eps = false;
@@ -313,15 +314,15 @@ struct Ops {
     dim3 grid(g().Lm * nft, 3 * nvec, nslots);
     a.pf_dist = 0;
     if (g().general) {
-      auto k = c->rare == 2   ? k_pencil<R, true, MODE, 2, DynGeom>
-               : c->rare == 1 ? k_pencil<R, true, MODE, 1, DynGeom>
+      auto k = c->rare_pen == 2   ? k_pencil<R, true, MODE, 2, DynGeom>
+               : c->rare_pen == 1 ? k_pencil<R, true, MODE, 1, DynGeom>
                               : k_pencil<R, true, MODE, 0, DynGeom>;
       allow_smem(k, sm);
       if (MODE == PEN_QBQ_CG && c->prefetch) a.pf_dist = wave_ctas(c, k, kPencilThreads, sm, 1);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
     } else {
-      auto k = c->rare == 2   ? k_pencil<R, false, MODE, 2, DynGeom>
-               : c->rare == 1 ? k_pencil<R, false, MODE, 1, DynGeom>
+      auto k = c->rare_pen == 2   ? k_pencil<R, false, MODE, 2, DynGeom>
+               : c->rare_pen == 1 ? k_pencil<R, false, MODE, 1, DynGeom>
                               : k_pencil<R, false, MODE, 0, DynGeom>;
       if constexpr (kStatPen<R, MODE> && sizeof(R) == 4)
         if (c->stat96) k = k_pencil<R, false, MODE, 0, Stat96>;
@@ -406,7 +407,8 @@ static int setup_geom(fame_ctx* c) {
     set_err(err);
     return rc;
   }
-  c->rare = geom_level(g);
+  c->rare = plane_level(g);
+  c->rare_pen = pencil_level(g);
   c->plane_threads32 = plane_threads_rule<float>(g, c->rare);
   c->plane_threads = plane_threads_rule<double>(g, c->rare);
   c->stat96 = !g.general && g.Nx == 96 && g.Ny == 96 && g.Nz == 96;
@@ -1339,7 +1341,8 @@ int fame_set_option(fame_ctx* c, const char* name, int value) {
   } else if (n == "radix_order" && value >= 0 && value < kNumRadixOrders) {
     Geom g;
     std::string err;
-    if (layout_geom(c->lat, g, 1L << 28, err, value) != FAME_OK || geom_level(g) != c->rare) {
+    if (layout_geom(c->lat, g, 1L << 28, err, value) != FAME_OK || plane_level(g) != c->rare ||
+        pencil_level(g) != c->rare_pen) {
       set_err("radix order " + std::to_string(value) + " gives no plan for this grid");
       return FAME_ERR_BAD_INPUT;
     }
@@ -1385,7 +1388,7 @@ int fame_get_option(fame_ctx* c, const char* name, int* value) {
   } else if (n == "grid_x" || n == "grid_y" || n == "grid_z") {
     *value = n == "grid_x" ? c->g.Nx : n == "grid_y" ? c->g.Ny : c->g.Nz;
   } else if (n == "level") {
-    *value = c->rare;
+    *value = std::max(c->rare, c->rare_pen);
   } else if (n == "plan_signature") {
     // the radix lists of the three axis plans, hashed (equal plans, equal values)
     unsigned h = 2166136261u;
