@@ -67,6 +67,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geom& g = a.g;
   const int Lf = GP::Lf(g), Lm = GP::Lm(g), S = GP::S(g), P = GP::P(g);
+  const Div dlf(Lf);  // row of plane element e: e / Lf (folds to a constant for static geometries)
   cplx<R>* plane = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* twf = plane + Lm * S;  // plane rows have the odd pitch S >= Lf
   cplx<R>* twm = twf + Lf;
@@ -224,7 +225,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       const int e = eb + k * NT;
       if (e >= e1) break;
       const int fi = s * P + e;
-      const int m = e / Lf, f = e - m * Lf;
+      const int m = GP::kStatic ? e / Lf : (int)dlf.q(e), f = e - m * Lf;
       cplx<R> v[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
       if (fi >= off) {
         const long i = fi - off;
@@ -314,7 +315,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       // x D_kz(x,y,z) after the z (fast) pass (FAME_FFT_CUDA.cu:109, kernel :283-317),
       // x D_ky(x,y) after the y (mid) pass (FAME_FFT_CUDA.cu:115, kernel :198-234)
       for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
-        const int m = e / Lf, f = e - m * Lf;
+        const int m = GP::kStatic ? e / Lf : (int)dlf.q(e), f = e - m * Lf;
         const int q = m * S + f;
         plane[q] = cmul(plane[q], ax == 0 ? dkz_at<R>(g, tab, s, m, f) : cvt<R>(tab[g.oDky + s * g.Ny + m]));
       }
@@ -323,7 +324,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   }
   cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
   for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
-    const int m = e / Lf;
+    const int m = GP::kStatic ? e / Lf : (int)dlf.q(e);
     T[e] = plane[e + m * (S - Lf)];
   }
 }
@@ -615,6 +616,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geom& g = a.g;
   const int Lf = GP::Lf(g), Lm = GP::Lm(g), S = GP::S(g), P = GP::P(g);
+  const Div dlf(Lf);  // row of plane element e: e / Lf (folds to a constant for static geometries)
   cplx<R>* plane = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* twf = plane + Lm * S;  // plane rows have the odd pitch S >= Lf
   cplx<R>* twm = twf + Lf;
@@ -673,7 +675,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
   const cplx<R> lz = GEN ? mk<R>(0, 0) : cvt<R>(tab[g.oLz + s]);
   const cplx<R>* T = a.T + (long)(slot * a.vec_per_slot + vec) * a.fstride + (long)comp * g.N + (long)s * P;
   for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
-    const int m = e / Lf;
+    const int m = GP::kStatic ? e / Lf : (int)dlf.q(e);
     cp_async_elem(plane + e + m * (S - Lf), T + e);
   }
   __shared__ R s_step;
@@ -699,7 +701,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
     const bool fast = GEN ? ax == 1 : ax == 0;
     if constexpr (GEN) {
       for (int e = threadIdx.x; e < P; e += GP::plane_threads()) {
-        const int m = e / Lf, f = e - m * Lf;
+        const int m = GP::kStatic ? e / Lf : (int)dlf.q(e), f = e - m * Lf;
         const int q = m * S + f;
         plane[q] = cmul(plane[q], ax == 0 ? cvt<R>(cconj(tab[g.oDky + s * g.Ny + m]))
                                           : cconj(dkz_at<R>(g, tab, s, m, f)));
@@ -732,7 +734,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       const int fi = s * P + e;
       if (e < e1 && fi >= off) {
         const long i = fi - off;
-        const int m = e / Lf, q = m * S + (e - m * Lf);
+        const int m = GP::kStatic ? e / Lf : (int)dlf.q(e), q = m * S + (e - m * Lf);
 #pragma unroll
         for (int c = 0; c < 3; c++) t[k][c] = src[c][q];
         if constexpr (EPI == EPI_CG) {
@@ -753,7 +755,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads
       const int fi = s * P + e;
       if (e >= e1 || fi < off) continue;
       const long i = fi - off;
-      const int m = e / Lf, f = e - m * Lf;
+      const int m = GP::kStatic ? e / Lf : (int)dlf.q(e), f = e - m * Lf;
       cplx<R> Lx, Ly, Lz;
       lam_elem<R, GEN>(g, tab, lx, ly, lz, s, m, f, Lx, Ly, Lz);
       cplx<R> Pc[6];
