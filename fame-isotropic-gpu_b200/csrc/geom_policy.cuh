@@ -52,6 +52,20 @@ template <typename R> struct SPenEmax;
 template <> struct SPenEmax<float> { static constexpr int v = 24; };
 template <> struct SPenEmax<double> { static constexpr int v = 12; };
 
+// DynGeom with the slow-axis length fixed at compile time: the pencil stage's
+// slow-axis transforms run the static plan (unrolled passes, constant strides and
+// twiddle indices); everything else stays runtime.  The solver uses it for the
+// pencils of runtime-geometry grids whose slow axis is one of the lengths
+// instantiated in ops_slow_static.cu.
+template <int LSL>
+struct DynGeomSlow : DynGeom {
+  template <typename R, int RARE>
+  __device__ __forceinline__ static void fft_slow(cplx<R>* b, const Geom&, const cplx<R>* tw, bool inv) {
+    constexpr int TW = PencilTW<R>::v;
+    sfft<R, LSL, TW, kPencilThreads, SPenEmax<R>::v>(b, 1, TW, tw, inv);
+  }
+};
+
 template <int LF, int LM, int LSL>
 struct StatGeom {
   static constexpr bool kStatic = true;

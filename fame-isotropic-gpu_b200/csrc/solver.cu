@@ -42,6 +42,7 @@ unsigned long long launches_ops_f64_simple_prime();
 unsigned long long launches_ops_f64_general_prime();
 unsigned long long launches_ops_stat96_f32();
 unsigned long long launches_ops_stat96_f64();
+unsigned long long launches_ops_slow_static();
 unsigned long long launches_material_locate();
 FAME_DEFINE_LAUNCH_GETTER(launches_solver)
 
@@ -317,6 +318,12 @@ struct Ops {
       auto k = c->rare_pen == 2   ? k_pencil<R, true, MODE, 2, DynGeom>
                : c->rare_pen == 1 ? k_pencil<R, true, MODE, 1, DynGeom>
                               : k_pencil<R, true, MODE, 0, DynGeom>;
+      if constexpr (!(sizeof(R) == 8 && MODE == PEN_QBQ_CG))
+        if (c->rare_pen == 0) {  // static slow-axis plans (ops_slow_static.cu)
+          if (g().Ls == 48) k = k_pencil<R, true, MODE, 0, DynGeomSlow<48>>;
+          if (g().Ls == 64) k = k_pencil<R, true, MODE, 0, DynGeomSlow<64>>;
+          if (g().Ls == 128) k = k_pencil<R, true, MODE, 0, DynGeomSlow<128>>;
+        }
       allow_smem(k, sm);
       if (MODE == PEN_QBQ_CG && c->prefetch) a.pf_dist = wave_ctas(c, k, kPencilThreads, sm, 1);
       P.launch(k, grid, dim3(kPencilThreads), sm, a);
@@ -1424,7 +1431,7 @@ int fame_launch_count(fame_ctx* c, unsigned long long* out) {
            launches_ops_f64_simple_rare() + launches_ops_f64_general_rare() + launches_ops_f32_simple_prime() +
            launches_ops_f32_general_prime() + launches_ops_f64_simple_prime() + launches_ops_f64_general_prime() +
            launches_ops_stat96_f32() +
-           launches_ops_stat96_f64() + launches_material_locate();
+           launches_ops_stat96_f64() + launches_ops_slow_static() + launches_material_locate();
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;
