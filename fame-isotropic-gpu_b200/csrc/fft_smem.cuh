@@ -601,35 +601,39 @@ __device__ __forceinline__ void fft_lines(cplx<R>* buf, const AxisPlan P, LineSe
 // ---------------------------------------------------------------- compile-time plans
 // Static plans: a two-pass split n = r0 * r1 with both radices in {4, 8, 12}
 // when one exists (fewest passes, each a single register-staged round), else the
-// greedy factorisation into 8, 4, 2, 5, 3 of the runtime plans.
+// greedy factorisation into 8, 4, 2, 5, 3, 7, 11, 13 and then the remaining prime
+// factors (>= 17), as the runtime plans do.
 constexpr int kSplit[][2] = {{8, 12}, {12, 8}, {8, 8}, {4, 12}, {12, 12}, {4, 8}, {8, 4}, {4, 4}};
+constexpr int kSRadix[8] = {8, 4, 2, 5, 3, 7, 11, 13};
 constexpr int splan_split(int n) {
   for (int i = 0; i < (int)(sizeof(kSplit) / sizeof(kSplit[0])); i++)
     if (kSplit[i][0] * kSplit[i][1] == n) return i;
   return -1;
 }
-constexpr int splan_count(int n) {
-  if (splan_split(n) >= 0) return 2;
+// radix of pass p (p < 0: the number of passes; 0 when n does not factor)
+constexpr int splan_walk(int n, int p) {
   int c = 0;
-  const int rs[5] = {8, 4, 2, 5, 3};
-  for (int i = 0; i < 5; i++)
-    while (n % rs[i] == 0) {
-      n /= rs[i];
+  for (int i = 0; i < 8; i++)
+    while (n % kSRadix[i] == 0) {
+      if (c == p) return kSRadix[i];
+      n /= kSRadix[i];
       c++;
     }
-  return n == 1 ? c : -1;
+  for (int q = 17; n > 1 && q <= n; q++)
+    while (n % q == 0) {
+      if (c == p) return q;
+      n /= q;
+      c++;
+    }
+  return p < 0 ? c : 0;
+}
+constexpr int splan_count(int n) {
+  if (splan_split(n) >= 0) return 2;
+  return splan_walk(n, -1);
 }
 constexpr int splan_radix(int n, int p) {
   if (splan_split(n) >= 0) return kSplit[splan_split(n)][p];
-  const int rs[5] = {8, 4, 2, 5, 3};
-  int c = 0;
-  for (int i = 0; i < 5; i++)
-    while (n % rs[i] == 0) {
-      if (c == p) return rs[i];
-      n /= rs[i];
-      c++;
-    }
-  return 0;
+  return splan_walk(n, p);
 }
 
 // One radix-RAD pass with the line length N, line count NL and thread count T
@@ -700,11 +704,18 @@ constexpr int smaxb(int N, int NL, int T, int EMAX, int RAD) {
 
 template <typename R, int N, int NL, int T, int EMAX, int P = 0, int NS = 1>
 __device__ __forceinline__ void sfft(cplx<R>* buf, int ls, int es, const cplx<R>* tw, bool inv) {
-  static_assert(splan_count(N) > 0, "line length must factor into 2, 3, 4, 5, 8, 12");
+  static_assert(N == 1 || splan_count(N) > 0, "line length without a static plan");
   if constexpr (P < splan_count(N)) {
     constexpr int RAD = splan_radix(N, P);
-    constexpr int MB = smaxb(N, NL, T, EMAX, RAD);
-    spass<R, N, NL, T, NS, RAD, MB>(buf, ls, es, tw, inv);
+    if constexpr (RAD >= 17) {
+      // a prime factor >= 17: the symmetric-pair pass, its sizes compile-time constants
+      const LineSet L{NL, ls, es};
+      if (!prime_pass<R, PrimeBlock<R>::mu, PrimeBlock<R>::ml>(buf, N, RAD, NS, L, tw, inv))
+        generic_pass<R, EMAX>(buf, N, RAD, NS, L, tw, inv);
+    } else {
+      constexpr int MB = smaxb(N, NL, T, EMAX, RAD);
+      spass<R, N, NL, T, NS, RAD, MB>(buf, ls, es, tw, inv);
+    }
     sfft<R, N, NL, T, EMAX, P + 1, NS * RAD>(buf, ls, es, tw, inv);
   }
 }

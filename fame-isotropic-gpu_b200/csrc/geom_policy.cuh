@@ -22,6 +22,8 @@ struct DynGeom {
   // three pencil CTAs (85 registers), except that plane kernels with the prime
   // pass (RARE 2), whose MU x ML accumulator block needs more, take one.
   __device__ __forceinline__ static int plane_threads() { return blockDim.x; }
+  // plane CTAs per SM the register budget is sized for (launch bounds)
+  template <typename R, int RARE> static constexpr int plane_min_blocks() { return RARE >= 2 ? 1 : 2; }
   __device__ __forceinline__ static int Lf(const Geom& g) { return g.Lf; }
   __device__ __forceinline__ static int Lm(const Geom& g) { return g.Lm; }
   __device__ __forceinline__ static int Ls(const Geom& g) { return g.Ls; }
@@ -66,6 +68,26 @@ struct DynGeomSlow : DynGeom {
   }
 };
 
+// DynGeom with the two plane axes' lengths fixed at compile time: the plane stages'
+// fast- and mid-axis transforms run static plans (spass, and the prime pass with
+// constant sizes); T threads per plane CTA, MB CTAs per SM in the register budget.
+// Index arithmetic outside the transforms stays runtime.  The solver uses it for the
+// plane stages of the runtime-geometry grids instantiated in ops_plane_static.cu.
+template <int LF, int LM, int T, int MB>
+struct DynGeomPlane : DynGeom {
+  static constexpr int kMaxPlaneThreads = T;
+  __device__ __forceinline__ static constexpr int plane_threads() { return T; }
+  template <typename R, int RARE> static constexpr int plane_min_blocks() { return MB; }
+  template <typename R, int RARE>
+  __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom&, bool fast, const cplx<R>* tw,
+                                                   bool inv) {
+    if (fast)
+      sfft<R, LF, LM, T, SEmax<R>::v>(b, LF | 1, 1, tw, inv);
+    else
+      sfft<R, LM, LF, T, SEmax<R>::v>(b, 1, LF | 1, tw, inv);
+  }
+};
+
 template <int LF, int LM, int LSL>
 struct StatGeom {
   static constexpr bool kStatic = true;
@@ -76,6 +98,7 @@ struct StatGeom {
   // two FP32 plane CTAs per SM (80 registers), one FP64 plane CTA; three FP32 and
   // two FP64 pencil CTAs
   __device__ __forceinline__ static constexpr int plane_threads() { return kStatPlaneThreads; }
+  template <typename R, int RARE> static constexpr int plane_min_blocks() { return sizeof(R) == 4 ? 2 : 1; }
   __device__ __forceinline__ static constexpr int Lf(const Geom&) { return LF; }
   __device__ __forceinline__ static constexpr int Lm(const Geom&) { return LM; }
   __device__ __forceinline__ static constexpr int Ls(const Geom&) { return LSL; }
@@ -106,5 +129,10 @@ struct StatGeom {
 };
 
 using Stat96 = StatGeom<96, 96, 96>;
+// static plane plans of the general-lattice benchmark grids (fast, mid, threads, CTAs per SM)
+using PlaneFcc64 = DynGeomPlane<52, 55, 256, 2>;
+using PlaneBcc48 = DynGeomPlane<39, 45, 256, 2>;
+using PlaneHex128f = DynGeomPlane<92, 107, 256, 2>;
+using PlaneHex128d = DynGeomPlane<92, 107, 512, 1>;
 
 }  // namespace fame

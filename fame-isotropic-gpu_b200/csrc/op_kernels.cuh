@@ -60,7 +60,7 @@ __device__ __forceinline__ bool plane_vec_range(int P, int s, int comp, const Sl
 
 // One cluster = 3 CTAs = the 3 components of plane s.  grid = (3*Ls, vec_per_slot, nslots)
 template <typename R, bool GEN, int IN, bool PR, int RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::kStatic ? (sizeof(R) == 4 ? 2 : 1) : (RARE >= 2 ? 1 : 2))
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::template plane_min_blocks<R, RARE>())
     k_plane_inv(PlaneInArgs<R> a) {
   FAME_COUNT_LAUNCH();
   if ((threadIdx.x | blockIdx.x | blockIdx.y | blockIdx.z) == 0) set_cond(a.reset, 0);
@@ -610,7 +610,7 @@ __device__ __forceinline__ void plane_fwd_decide(const PlaneOutArgs<R>& a) {
 }
 
 template <typename R, bool GEN, int EPI, bool PR, int RARE, class GP>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::kStatic ? (sizeof(R) == 4 ? 2 : 1) : (RARE >= 2 ? 1 : 2))
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(GP::kMaxPlaneThreads, GP::template plane_min_blocks<R, RARE>())
     k_plane_fwd(PlaneOutArgs<R> a) {
   FAME_COUNT_LAUNCH();
   extern __shared__ __align__(16) unsigned char smem_raw[];

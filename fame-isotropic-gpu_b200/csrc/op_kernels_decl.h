@@ -32,6 +32,13 @@ template <typename R, bool GEN, int EPI, bool PR, int RARE, class GP> __global__
 template <typename R, int IN, bool PR>
 constexpr bool kStatInv = !PR && (IN == IN_CG || IN == IN_VEC || (IN == IN_REFINE && sizeof(R) == 8));
 template <typename R, int MODE> constexpr bool kStatPen = MODE == PEN_QBQ || (MODE == PEN_QBQ_CG && sizeof(R) == 4);
+// combinations instantiated with static plane plans on runtime geometries
+// (ops_plane_static.cu)
+template <typename R, int IN, bool PR>
+constexpr bool kPlanInv = (IN == IN_CG && !PR) || IN == IN_VEC || (IN == IN_REFINE && !PR && sizeof(R) == 8);
+template <typename R, int EPI, bool PR>
+constexpr bool kPlanFwd = EPI == EPI_OUT || (!PR && ((EPI == EPI_CGR && sizeof(R) == 4) ||
+                                                      ((EPI == EPI_CG || EPI == EPI_RESID) && sizeof(R) == 8)));
 template <typename R, int EPI, bool PR>
 constexpr bool kStatFwd = !PR && ((EPI == EPI_CG && sizeof(R) == 8) || (EPI == EPI_CGR && sizeof(R) == 4) || EPI == EPI_OUT ||
                                   (EPI == EPI_RESID && sizeof(R) == 8));

@@ -43,6 +43,7 @@ unsigned long long launches_ops_f64_general_prime();
 unsigned long long launches_ops_stat96_f32();
 unsigned long long launches_ops_stat96_f64();
 unsigned long long launches_ops_slow_static();
+unsigned long long launches_ops_plane_static();
 unsigned long long launches_material_locate();
 FAME_DEFINE_LAUNCH_GETTER(launches_solver)
 
@@ -90,6 +91,7 @@ struct fame_ctx {
   std::map<const void*, int> waves;  // resident CTAs of a stage kernel on the device
   int rare = 0;      // fft_lines level the plane axes need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   int rare_pen = 0;  // the same for the pencil (slow) axis
+  int static_planes = 1;  // static plane plans where instantiated (option "static_planes")
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   int loop_cap = 0;     // fame_set_loop_cap: bound on every device loop's trips (0: defaults)
   bool have_eps = false;
@@ -214,6 +216,17 @@ struct Ops {
 
   template <typename R> const cplx<R>* tw() const;
 
+  // static plane plans (ops_plane_static.cu) for the runtime-geometry grids they cover:
+  // 1 FCC 64x55x52, 2 BCC 48x45x39, 3 hexagonal 128x107x92, 0 none (or switched off)
+  int plane_plan() const {
+    const Geom& q = g();
+    if (!q.general || !c->static_planes) return 0;
+    if (q.Lf == 52 && q.Lm == 55) return 1;
+    if (q.Lf == 39 && q.Lm == 45) return 2;
+    if (q.Lf == 92 && q.Lm == 107) return 3;
+    return 0;
+  }
+
   // partial sums per slot of the fused FP32 CG kernels: the pencil stage's <p, Ap>
   // (one per CTA of a slot), then the forward plane stage's ||r||^2
   int cg_pen_parts() const { return 3 * g().Lm * ((g().Lf + pencil_tw<float>() - 1) / pencil_tw<float>()); }
@@ -267,10 +280,22 @@ struct Ops {
       auto k = c->rare == 2   ? k_plane_inv<R, true, IN, PR, 2, DynGeom>
                : c->rare == 1 ? k_plane_inv<R, true, IN, PR, 1, DynGeom>
                               : k_plane_inv<R, true, IN, PR, 0, DynGeom>;
+      int nt = c->template plane_nt<R>();
+      if constexpr (kPlanInv<R, IN, PR>) {
+        const int pp = plane_plan();
+        if (pp == 1) k = k_plane_inv<R, true, IN, PR, 0, PlaneFcc64>, nt = PlaneFcc64::kMaxPlaneThreads;
+        if (pp == 2) k = k_plane_inv<R, true, IN, PR, 0, PlaneBcc48>, nt = PlaneBcc48::kMaxPlaneThreads;
+        if (pp == 3) {
+          if constexpr (sizeof(R) == 4)
+            k = k_plane_inv<R, true, IN, PR, 0, PlaneHex128f>, nt = PlaneHex128f::kMaxPlaneThreads;
+          else
+            k = k_plane_inv<R, true, IN, PR, 0, PlaneHex128d>, nt = PlaneHex128d::kMaxPlaneThreads;
+        }
+      }
       allow_smem(k, sm);
-      a.pf_dist = IN == IN_CG && c->prefetch ? wave_ctas(c, k, c->template plane_nt<R>(), sm, 3) : 0;
+      a.pf_dist = IN == IN_CG && c->prefetch ? wave_ctas(c, k, nt, sm, 3) : 0;
       a.self_pf = c->self_prefetch;
-      P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
+      P.launch(k, grid, dim3(nt), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_inv<R, false, IN, PR, 2, DynGeom>
                : c->rare == 1 ? k_plane_inv<R, false, IN, PR, 1, DynGeom>
@@ -381,10 +406,22 @@ struct Ops {
       auto k = c->rare == 2   ? k_plane_fwd<R, true, EPI, PR, 2, DynGeom>
                : c->rare == 1 ? k_plane_fwd<R, true, EPI, PR, 1, DynGeom>
                               : k_plane_fwd<R, true, EPI, PR, 0, DynGeom>;
+      int nt = c->template plane_nt<R>();
+      if constexpr (kPlanFwd<R, EPI, PR>) {
+        const int pp = plane_plan();
+        if (pp == 1) k = k_plane_fwd<R, true, EPI, PR, 0, PlaneFcc64>, nt = PlaneFcc64::kMaxPlaneThreads;
+        if (pp == 2) k = k_plane_fwd<R, true, EPI, PR, 0, PlaneBcc48>, nt = PlaneBcc48::kMaxPlaneThreads;
+        if (pp == 3) {
+          if constexpr (sizeof(R) == 4)
+            k = k_plane_fwd<R, true, EPI, PR, 0, PlaneHex128f>, nt = PlaneHex128f::kMaxPlaneThreads;
+          else
+            k = k_plane_fwd<R, true, EPI, PR, 0, PlaneHex128d>, nt = PlaneHex128d::kMaxPlaneThreads;
+        }
+      }
       allow_smem(k, sm);
-      a.pf_dist = EPI == EPI_CGR && c->prefetch ? wave_ctas(c, k, c->template plane_nt<R>(), sm, 3) : 0;
+      a.pf_dist = EPI == EPI_CGR && c->prefetch ? wave_ctas(c, k, nt, sm, 3) : 0;
       a.self_pf = c->self_prefetch;
-      P.launch(k, grid, dim3(c->template plane_nt<R>()), sm, a);
+      P.launch(k, grid, dim3(nt), sm, a);
     } else {
       auto k = c->rare == 2   ? k_plane_fwd<R, false, EPI, PR, 2, DynGeom>
                : c->rare == 1 ? k_plane_fwd<R, false, EPI, PR, 1, DynGeom>
@@ -1345,6 +1382,8 @@ int fame_set_option(fame_ctx* c, const char* name, int value) {
     c->prefetch = value;
   } else if (n == "self_prefetch" && (value == 0 || value == 1)) {
     c->self_prefetch = value;
+  } else if (n == "static_planes" && (value == 0 || value == 1)) {
+    c->static_planes = value;
   } else if (n == "radix_order" && value >= 0 && value < kNumRadixOrders) {
     Geom g;
     std::string err;
@@ -1382,6 +1421,8 @@ int fame_get_option(fame_ctx* c, const char* name, int* value) {
     *value = c->prefetch;
   } else if (n == "self_prefetch") {
     *value = c->self_prefetch;
+  } else if (n == "static_planes") {
+    *value = c->static_planes;
   } else if (n == "radix_order") {
     *value = c->radix_order;
   } else if (n == "plane_threads32") {
@@ -1431,7 +1472,8 @@ int fame_launch_count(fame_ctx* c, unsigned long long* out) {
            launches_ops_f64_simple_rare() + launches_ops_f64_general_rare() + launches_ops_f32_simple_prime() +
            launches_ops_f32_general_prime() + launches_ops_f64_simple_prime() + launches_ops_f64_general_prime() +
            launches_ops_stat96_f32() +
-           launches_ops_stat96_f64() + launches_ops_slow_static() + launches_material_locate();
+           launches_ops_stat96_f64() + launches_ops_slow_static() + launches_ops_plane_static() +
+           launches_material_locate();
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;
