@@ -504,6 +504,7 @@ __device__ __forceinline__ bool prime_pass(cplx<R>* buf, int n, int r, int Ns, L
       for (int m = 0; m < MU; m++) idx[m] = 0;
       const cplx<R>* pp = buf + (l0 + lt) * L.ls + j * L.es;
       const cplx<R>* pq = pp + r * dstep;
+#pragma unroll 4  // loads of the next s issue under the FMAs of this one
       for (int s = 1; s <= H; s++) {
         pp += dstep;
         pq -= dstep;
