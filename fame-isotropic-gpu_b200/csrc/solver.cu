@@ -16,6 +16,7 @@
 #include <chrono>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <utility>
@@ -92,6 +93,15 @@ struct fame_ctx {
   int rare = 0;      // fft_lines level the plane axes need: 0 radix 2-8, 1 + 7/11/13, 2 + primes >= 17
   int rare_pen = 0;  // the same for the pencil (slow) axis
   int static_planes = 1;  // static plane plans where instantiated (option "static_planes")
+  // An automatic batch of at least 4 k-points per lane is split into `lanes` contiguous
+  // blocks solved concurrently, each by a lane context on its own stream and host
+  // thread, so one block's FP64 refinement and Lanczos phases run under another's FP32
+  // CG (option "lanes").  Lane 0 is this context; the others share its lattice, its
+  // permittivity (copied device to device when eps_ver changes) and its options.
+  int lanes = 2;
+  int eps_ver = 0;
+  std::vector<fame_ctx*> lane_ctx;
+  std::vector<int> lane_eps_ver;
   bool stat96 = false;  // Simple lattice on a 96^3 grid: compile-time geometry kernels
   int loop_cap = 0;     // fame_set_loop_cap: bound on every device loop's trips (0: defaults)
   bool have_eps = false;
@@ -942,6 +952,8 @@ int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out) {
 
 void fame_ctx_destroy(fame_ctx* c) {
   if (!c) return;
+  for (fame_ctx* l : c->lane_ctx) fame_ctx_destroy(l);
+  c->lane_ctx.clear();
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->progs.clear();
@@ -1020,6 +1032,7 @@ int fame_set_eps(fame_ctx* c, const double* B) {
     return FAME_ERR_CUDA;
   }
   c->have_eps = true;
+  c->eps_ver++;
   return FAME_OK;
 }
 
@@ -1037,9 +1050,10 @@ int fame_set_material(fame_ctx* c, const int* binout, int material_num, const do
   return fame_set_eps(c, B.data());
 }
 
-int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solver_params* prm,
-                       double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
-                       double* evec_out, fame_kcounters* counters) {
+// One context's solve of nk k-points in batches (the body of fame_solve_kpoints).
+static int solve_batched(fame_ctx* c, const double* k_xyz, int nk, const fame_solver_params* prm,
+                         double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
+                         double* evec_out, fame_kcounters* counters) {
   if (!c || !k_xyz || !prm || !freq_out || nk <= 0) {
     set_err("null or empty argument");
     return FAME_ERR_BAD_INPUT;
@@ -1234,6 +1248,97 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
   return rc_all;
 }
 
+// Lane contexts 1 .. G-1 of c: created on first use with c's lattice, given c's
+// permittivity (device to device) whenever it changed, and c's execution options.
+static int sync_lanes(fame_ctx* c, int G) {
+  while ((int)c->lane_ctx.size() < G - 1) {
+    fame_ctx* l = nullptr;
+    const int rc = fame_ctx_create(c->device, &c->lat, &l);
+    if (rc != FAME_OK) return rc;
+    c->lane_ctx.push_back(l);
+    c->lane_eps_ver.push_back(-1);
+  }
+  for (int i = 0; i < G - 1; i++) {
+    fame_ctx* l = c->lane_ctx[i];
+    if (c->lane_eps_ver[i] != c->eps_ver) {
+      const int rc = fame_set_eps_device(l, c->B64.p);
+      if (rc != FAME_OK) return rc;
+      c->lane_eps_ver[i] = c->eps_ver;
+    }
+    const struct {
+      const char* name;
+      int want, have;
+    } opts[] = {{"prefetch", c->prefetch, l->prefetch},
+                {"self_prefetch", c->self_prefetch, l->self_prefetch},
+                {"static_planes", c->static_planes, l->static_planes},
+                {"radix_order", c->radix_order, l->radix_order},
+                {"plane_threads32", c->threads32_opt, l->threads32_opt},
+                {"plane_threads64", c->threads64_opt, l->threads64_opt}};
+    for (const auto& o : opts)
+      if (o.want != o.have) {
+        const int rc = fame_set_option(l, o.name, o.want);
+        if (rc != FAME_OK) return rc;
+      }
+    l->loop_cap = c->loop_cap;
+  }
+  return FAME_OK;
+}
+
+int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solver_params* prm,
+                       double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
+                       double* evec_out, fame_kcounters* counters) {
+  int G = 1;
+  if (c && k_xyz && prm && freq_out && nk > 0 && c->have_eps && prm->batch == 0 &&
+      !(prm->want_vectors && !evec_out) && c->lanes > 1)
+    G = std::min(c->lanes, nk / 4);
+  if (G <= 1)
+    return solve_batched(c, k_xyz, nk, prm, freq_out, relres_out, relerr_out, resabs_out, evec_out, counters);
+  std::vector<fame_solver_params> pl(G, *prm);
+  try {
+    FAME_CK(cudaSetDevice(c->device));
+    const int rc = sync_lanes(c, G);
+    if (rc != FAME_OK) return rc;
+    // each lane's batch: its k-points, at most what 60% of the free memory holds over
+    // the G lanes (lane contexts allocate their workspace on their first solve)
+    size_t free_b = 0, total_b = 0;
+    FAME_CK(cudaMemGetInfo(&free_b, &total_b));
+    const double per = slot_bytes(c, prm->nstep, prm->nwant, prm->precision == FAME_MIXED,
+                                  prm->want_vectors || resabs_out);
+    const int cap = (int)std::max(1.0, std::min(64.0, floor(0.6 * (double)free_b / (G * per))));
+    for (int i = 0; i < G; i++) pl[i].batch = std::min(cap, (int)((long)nk * (i + 1) / G - (long)nk * i / G));
+  } catch (const CudaError& e) {
+    set_err(e.what());
+    return FAME_ERR_CUDA;
+  }
+  const size_t nw = (size_t)prm->nwant, n3 = 3 * (size_t)c->g.N;
+  std::vector<int> rcs(G, FAME_OK);
+  std::vector<std::string> errs(G);
+  auto run = [&](int i) {
+    fame_ctx* l = i == 0 ? c : c->lane_ctx[i - 1];
+    const long a = (long)nk * i / G, b = (long)nk * (i + 1) / G;
+    cudaSetDevice(c->device);
+    rcs[i] = solve_batched(l, k_xyz + 3 * a, (int)(b - a), &pl[i], freq_out + a * nw,
+                           relres_out ? relres_out + a * nw : nullptr, relerr_out ? relerr_out + a * nw : nullptr,
+                           resabs_out ? resabs_out + a * nw : nullptr, evec_out ? evec_out + a * nw * n3 * 2 : nullptr,
+                           counters ? counters + a : nullptr);
+    if (rcs[i] != FAME_OK) errs[i] = fame_last_error();
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < G; i++) th.emplace_back(run, i);
+  run(0);
+  for (auto& t : th) t.join();
+  // a failure outranks a k-point that did not converge
+  int out = FAME_OK;
+  for (int pass = 0; pass < 2 && out == FAME_OK; pass++)
+    for (int i = 0; i < G; i++)
+      if (rcs[i] != FAME_OK && (pass == 1 || rcs[i] != FAME_ERR_NO_CONVERGENCE)) {
+        out = rcs[i];
+        set_err(errs[i]);
+        break;
+      }
+  return out;
+}
+
 int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, int precision,
                const fame_solver_params* prm, int* Nd_out) {
   if (!c || !k || !in || !out) {
@@ -1384,6 +1489,9 @@ int fame_set_option(fame_ctx* c, const char* name, int value) {
     c->self_prefetch = value;
   } else if (n == "static_planes" && (value == 0 || value == 1)) {
     c->static_planes = value;
+  } else if (n == "lanes" && value >= 1 && value <= 8) {
+    c->lanes = value;
+    return FAME_OK;  // no recorded graph changes
   } else if (n == "radix_order" && value >= 0 && value < kNumRadixOrders) {
     Geom g;
     std::string err;
@@ -1423,6 +1531,8 @@ int fame_get_option(fame_ctx* c, const char* name, int* value) {
     *value = c->self_prefetch;
   } else if (n == "static_planes") {
     *value = c->static_planes;
+  } else if (n == "lanes") {
+    *value = c->lanes;
   } else if (n == "radix_order") {
     *value = c->radix_order;
   } else if (n == "plane_threads32") {
@@ -1666,6 +1776,7 @@ int fame_set_eps_device(fame_ctx* c, const double* B) {
     return FAME_ERR_CUDA;
   }
   c->have_eps = true;
+  c->eps_ver++;
   return FAME_OK;
 }
 

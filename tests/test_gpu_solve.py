@@ -76,6 +76,32 @@ def test_graph_and_host_driven_agree_and_batches_are_independent():
     assert np.max(np.abs(a["freq"] - c["freq"])) < 1e-12
 
 
+def test_concurrent_lanes_match_a_single_batch():
+    """An automatic batch of 8 or more k-points runs as two concurrent lanes (contiguous
+    blocks, one lane context each); the option lanes = 1 solves them as one batch.  Both
+    give the reference's frequencies and agree to 1e-12; a permittivity change reaches
+    the lane contexts."""
+    par = load_pre("sc16")
+    k, fr, _ = _ref("sc16")
+    idx = np.arange(8) % len(k)
+    ctx = _ctx(par)
+    assert ctx.get_option("lanes") == 2
+    two = ctx.solve(k[idx], nwant=10, precision=fb.MIXED, **TOL)
+    ctx.set_option("lanes", 1)
+    one = ctx.solve(k[idx], nwant=10, precision=fb.MIXED, **TOL)
+    assert two["rc"] == fb.OK and one["rc"] == fb.OK
+    assert _relerr(two["freq"], fr[idx]) < 1e-6
+    assert np.max(np.abs(two["freq"] - one["freq"]) / np.maximum(one["freq"], 1e-300)) < 1e-12
+    # a new permittivity (uniform 2) reaches every lane: all k-points see the same medium
+    ctx.set_option("lanes", 2)
+    ctx.set_eps(np.full(3 * par["N"], 2.0))
+    u2 = ctx.solve(k[idx], nwant=10, precision=fb.MIXED, **TOL)
+    ctx.set_option("lanes", 1)
+    u1 = ctx.solve(k[idx], nwant=10, precision=fb.MIXED, **TOL)
+    assert np.max(np.abs(u2["freq"] - u1["freq"]) / np.maximum(u1["freq"], 1e-300)) < 1e-12
+    assert np.max(np.abs(u2["freq"] - two["freq"])) > 1e-3
+
+
 def test_eigenvectors_satisfy_the_curl_equation():
     """Independent check: sparse curl (FAME_Matrix_Curl.cpp semantics) on E."""
     par = load_pre("sc16")
