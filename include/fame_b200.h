@@ -191,8 +191,18 @@ int fame_set_loop_cap(fame_ctx* ctx, int max_trips);
  *   "plane_threads32", "plane_threads64": threads of a runtime-geometry plane CTA in the
  *                      FP32 / FP64 kernels, a multiple of 32 in 64..512, or 0 for the
  *                      built-in rule.
+ *   "self_prefetch"    1 (default): the CG plane stages prefetch their own operands into L2
+ *                      at the CTA's start; 0: off.
+ *   "static_planes"    1 (default): the plane stages of the FCC 64x55x52, BCC 48x45x39 and
+ *                      hexagonal 128x107x92 grids run compile-time FFT plans (fixed CTA
+ *                      sizes; the plane-thread options do not apply to them); 0: runtime plans.
+ *   "lanes"            1..8 (default 2): fame_solve_kpoints with an automatic batch
+ *                      (params.batch 0), at least 4 k-points per lane and eigenvectors not
+ *                      kept on the device splits the k-points into this many contiguous
+ *                      blocks, each solved concurrently by a lane context (own stream, own
+ *                      host thread, this context's permittivity and options); 1: one batch.
  * Read-only (fame_get_option): "static96", "general", "grid_x", "grid_y", "grid_z",
- * "level" (the FFT pass level the grid needs).  fame_tune picks these options by timing.
+ * "level" (the FFT pass level the grid needs).  fame_tune picks the first four by timing.
  * Unknown names or values are FAME_ERR_BAD_INPUT.  No counterpart in the reference. */
 int fame_set_option(fame_ctx* ctx, const char* name, int value);
 int fame_get_option(fame_ctx* ctx, const char* name, int* value);
