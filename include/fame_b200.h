@@ -293,7 +293,10 @@ int fame_material_locate(int device, const fame_locate_geometry* geo, const fame
  * grids return FAME_ERR_UNSUPPORTED.  Every call shares that array and leaves its
  * contents behind (nothing in it has to start at zero); calls that can overlap in
  * time race on it, so the caller serialises them.  The first call on a device
- * looks up the array's address; make it before any stream capture. */
+ * looks up the array's address and keeps it for the life of the process; make it
+ * before any stream capture.  The address belongs to the device's primary context:
+ * calls from a non-primary (driver-API) context, or after cudaDeviceReset, are not
+ * supported. */
 int fame_qbq_static(const fame_lattice* lat, const double* k_xyz, const double* inv_b, const void* x, void* y,
                     void* stream);
 
