@@ -418,6 +418,7 @@ def run_ours(args):
             "config": bench_config(nk, ws),
             "run": {"precision": args.precision, "batch": args.batch or "auto", "graph": not args.no_graph,
                     "fft_plan": plan,
+                    "lanes": ctx.get_option("lanes") if not args.batch else 1,
                     "l2": "inputs exceed L2 per step (>1000 CG iterations per step)",
                     "vectors": "eigenvalues only (want_vectors 0); the reference arm's timed region also "
                                "restores E and copies it to the host (about 2% of its time)"},
