@@ -15,8 +15,8 @@
 //     left at the last wave vector, the profile table printed per wave vector;
 //   * Data_Omega_array.txt written by the reference's FAME_Create_Frequency_txt and,
 //     when Par.flag.save_eigen_vector is set, Data_EV_*.txt in FAME_Save_Eigenvector's
-//     format by fame_writer_start (formatted on all host threads, written while the
-//     next wave vector is solved);
+//     format by fame_write_eigenvectors (formatted on all host threads) on a
+//     background thread: one batch's files while the next batch is solved;
 //   * the sign convention of Check_Residual (FAME_Main_Code.cu:383-421): a frequency
 //     whose residual ||C^H C E - w^2 B E|| (E scaled as the reference restores it)
 //     exceeds 1e-10 is stored negated.  The residual comes from the solver's FP64
@@ -28,11 +28,16 @@
 // precision comes from the environment variable FAME_B200_PRECISION: "mixed"
 // (default: FP32 operator and CG with FP64 refinement, FP64 Lanczos) or "fp64".
 // Errors are printed with fame_last_error() and returned as the fame status.
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
+#include <unistd.h>
 
+#include <algorithm>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "FAME_Internal_Common.h"
@@ -122,22 +127,36 @@ int FAME_Main_Code(PAR Par, PROFILE* Profile) {
   const char* prec = getenv("FAME_B200_PRECISION");
   p.precision = (prec && !strcmp(prec, "fp64")) ? FAME_FP64 : FAME_MIXED;
   p.use_graph = 1;
-  // with eigenvectors to save, one wave vector per call keeps the host buffer at 3N x Nwant
+  // With eigenvectors to save, the wave vectors are solved in batches of `chunk` into
+  // two host buffers of chunk x Nwant x 3N complex values: the files of one batch are
+  // written on a background thread while the next batch is solved into the other
+  // buffer.  chunk: what a quarter of the available host memory holds for the two
+  // buffers, or the environment variable FAME_B200_SAVE_BATCH.
   const bool save = Par.flag.save_eigen_vector != 0;
   p.want_vectors = save ? 1 : 0;
-  const int chunk = save ? 1 : nk;
+  const size_t per_k = (size_t)Nwant * 3 * N * 2;  // doubles of one wave vector's eigenvectors
+  int chunk = nk;
+  if (save) {
+    const long pages = sysconf(_SC_AVPHYS_PAGES), psz = sysconf(_SC_PAGESIZE);
+    const double avail = pages > 0 && psz > 0 ? (double)pages * (double)psz : 8e9;
+    chunk = (int)std::max(1.0, std::min((double)nk, floor(0.25 * avail / (2.0 * per_k * sizeof(double)))));
+    const char* env = getenv("FAME_B200_SAVE_BATCH");
+    if (env && atoi(env) > 0) chunk = std::min(nk, atoi(env));
+  }
 
   std::vector<double> freq((size_t)nk * Nwant), relres((size_t)nk * Nwant), resabs((size_t)nk * Nwant);
   std::vector<fame_kcounters> cnt(nk);
-  // two eigenvector buffers: the files of wave vector i are written on a background
-  // thread (fame_writer_start) while wave vector i + 1 is solved into the other
   std::vector<double> evec[2];
   if (save)
-    for (auto& e : evec) e.resize((size_t)Nwant * 3 * N * 2);
-  fame_writer* writer = nullptr;
+    for (auto& e : evec) e.resize((size_t)chunk * per_k);
+  // the background writer of the last batch: writes its wave vectors' files in order
+  std::thread writer;
+  int writer_rc = FAME_OK;
+  std::string writer_err;
   auto finish_writer = [&]() -> int {
-    const int wrc = writer ? fame_writer_finish(writer) : FAME_OK;
-    writer = nullptr;
+    if (writer.joinable()) writer.join();
+    const int wrc = writer_rc;
+    writer_rc = FAME_OK;
     return wrc;
   };
   int status = FAME_OK;
@@ -150,9 +169,11 @@ int FAME_Main_Code(PAR Par, PROFILE* Profile) {
                             save ? ev.data() : nullptr, cnt.data() + k0);
     const double dt = now_s() - t0;
     if (rc != FAME_OK && rc != FAME_ERR_NO_CONVERGENCE) {
+      const std::string msg = fame_last_error();
       finish_writer();
       fame_ctx_destroy(ctx);
-      return fail(rc, "fame_solve_kpoints");
+      fprintf(stderr, "FAME_Main_Code: fame_solve_kpoints: %s\n", msg.c_str());
+      return rc;
     }
     if (rc != FAME_OK) status = rc;
     for (int i = k0; i < k0 + n; i++) {
@@ -170,26 +191,32 @@ int FAME_Main_Code(PAR Par, PROFILE* Profile) {
                relres[(size_t)i * Nwant + b]);
         if (res > 1e-10) f = -f;
       }
-      if (save) {
-        // Data_EV_*.txt as FAME_Save_Eigenvector writes them (FAME_Main_Code.cu:127), byte for byte
-        const int wrc = finish_writer();
-        if (wrc != FAME_OK) {
-          fame_ctx_destroy(ctx);
-          return fail(wrc, "fame_writer_finish");
-        }
-        const int src = fame_writer_start(nullptr, ev.data(), Nwant, 3LL * N, i, 0, &writer);
-        if (src != FAME_OK) {
-          fame_ctx_destroy(ctx);
-          return fail(src, "fame_writer_start");
-        }
-      }
       FAME_Print_Profile(*Profile);
+    }
+    if (save) {
+      // Data_EV_*.txt as FAME_Save_Eigenvector writes them (FAME_Main_Code.cu:127), byte
+      // for byte: the previous batch's writer has finished with the other buffer, this
+      // batch's files are written while the next batch solves
+      const int wrc = finish_writer();
+      if (wrc != FAME_OK) {
+        fame_ctx_destroy(ctx);
+        fprintf(stderr, "FAME_Main_Code: writing eigenvectors: %s\n", writer_err.c_str());
+        return wrc;
+      }
+      const double* evp = ev.data();
+      writer = std::thread([&writer_rc, &writer_err, evp, per_k, Nwant, N, k0, n]() {
+        for (int i = k0; i < k0 + n && writer_rc == FAME_OK; i++) {
+          writer_rc = fame_write_eigenvectors(nullptr, evp + (size_t)(i - k0) * per_k, Nwant, 3LL * N, i, 0);
+          if (writer_rc != FAME_OK) writer_err = fame_last_error();
+        }
+      });
     }
   }
   const int wrc = finish_writer();
   if (wrc != FAME_OK) {
     fame_ctx_destroy(ctx);
-    return fail(wrc, "fame_writer_finish");
+    fprintf(stderr, "FAME_Main_Code: writing eigenvectors: %s\n", writer_err.c_str());
+    return wrc;
   }
   FAME_Create_Frequency_txt(freq.data(), Nwant, Profile->idx);
   fame_ctx_destroy(ctx);

@@ -36,6 +36,6 @@ done
 g++ -c "$HERE/FAME_Main_Code_b200.cpp" -o "$OUT/obj/FAME_Main_Code_b200.o" $CXXFLAGS -include time.h &
 pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
-g++ -o "$OUT/fame_b200_main" "$OUT"/obj/*.o -L"$PKG" -lfame_b200 -Wl,-rpath,"\$ORIGIN/../.." \
+g++ -pthread -o "$OUT/fame_b200_main" "$OUT"/obj/*.o -L"$PKG" -lfame_b200 -Wl,-rpath,"\$ORIGIN/../.." \
   -L/usr/local/cuda/lib64 -lcudart -Wl,-rpath,/usr/local/cuda/lib64
 echo "built $OUT/fame_b200_main"

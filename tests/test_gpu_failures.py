@@ -93,3 +93,24 @@ def test_loop_cap_ends_the_solve_with_watchdog(precision):
     with pytest.raises(fb.FameError):
         ctx.set_loop_cap(-1)
     ctx.close()
+
+
+def test_a_failing_lane_ends_the_call_with_its_status():
+    """Eight k-points run as two concurrent lanes; a loop cap that runs out in both lanes
+    (lane contexts take the context's cap) ends the call with FAME_ERR_WATCHDOG and the
+    lane's message, and the context and its lanes solve normally once the cap is lifted."""
+    par, ctx = _ctx()
+    idx = np.arange(8) % len(par["kpoints"])
+    k = par["kpoints"][idx]
+    kw = dict(nwant=4, nstep=20, es_tol=1e-10, ls_tol=1e-10, precision=fb.MIXED)
+    assert ctx.get_option("lanes") == 2
+    ctx.set_loop_cap(3)
+    with pytest.raises(fb.FameError) as e:
+        ctx.solve(k, **kw)
+    assert e.value.code == fb.ERR_WATCHDOG
+    assert "trip cap" in str(e.value)
+    ctx.set_loop_cap(0)
+    out = ctx.solve(k, **kw)
+    assert out["rc"] == fb.OK
+    assert out["relres"].max() < 1e-6
+    ctx.close()
