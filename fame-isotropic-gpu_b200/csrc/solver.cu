@@ -1296,8 +1296,9 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
   std::vector<fame_solver_params> pl(G, *prm);
   try {
     FAME_CK(cudaSetDevice(c->device));
-    const int rc = sync_lanes(c, G);
-    if (rc != FAME_OK) return rc;
+    // without its lane contexts (say, no device memory for one) the call runs as one batch
+    if (sync_lanes(c, G) != FAME_OK)
+      return solve_batched(c, k_xyz, nk, prm, freq_out, relres_out, relerr_out, resabs_out, evec_out, counters);
     // each lane's batch: its k-points, at most what 60% of the free memory holds over
     // the G lanes (lane contexts allocate their workspace on their first solve)
     size_t free_b = 0, total_b = 0;
@@ -1491,6 +1492,12 @@ int fame_set_option(fame_ctx* c, const char* name, int value) {
     c->static_planes = value;
   } else if (n == "lanes" && value >= 1 && value <= 8) {
     c->lanes = value;
+    // lane contexts beyond the new count are released with their device memory
+    while ((int)c->lane_ctx.size() > value - 1) {
+      fame_ctx_destroy(c->lane_ctx.back());
+      c->lane_ctx.pop_back();
+      c->lane_eps_ver.pop_back();
+    }
     return FAME_OK;  // no recorded graph changes
   } else if (n == "radix_order" && value >= 0 && value < kNumRadixOrders) {
     Geom g;

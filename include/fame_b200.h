@@ -201,6 +201,9 @@ int fame_set_loop_cap(fame_ctx* ctx, int max_trips);
  *                      kept on the device splits the k-points into this many contiguous
  *                      blocks, each solved concurrently by a lane context (own stream, own
  *                      host thread, this context's permittivity and options); 1: one batch.
+ *                      Lowering the value frees the lane contexts (and their device memory)
+ *                      it no longer needs; a call whose lane contexts cannot be created
+ *                      runs as one batch.
  * Read-only (fame_get_option): "static96", "general", "grid_x", "grid_y", "grid_z",
  * "level" (the FFT pass level the grid needs).  fame_tune picks the first four by timing.
  * Unknown names or values are FAME_ERR_BAD_INPUT.  No counterpart in the reference. */
