@@ -888,13 +888,23 @@ static double slot_bytes(const fame_ctx* c, int nstep, int nwant, bool mixed, bo
 // k-points per batch.  The stage kernels of one k-point do not fill the GPU (a 96^3
 // plane stage is 96 three-CTA clusters, slightly more than fit at once), so several
 // k-points per launch pay: as many as 60% of the free device memory holds, at most 64.
+// Slots of workspace the context already holds for this configuration (0 if a solve
+// with it would have to reallocate).
+static int held_slots(const fame_ctx* c, int nstep, int nwant, bool mixed, bool vec) {
+  const bool fits = c->cap_nstep >= nstep && c->cap_nwant >= nwant && (!mixed || c->cap_mixed) && (!vec || c->cap_vec);
+  return fits ? c->cap_slots : 0;
+}
+
+// Automatic batch: what 60% of the free device memory holds, or the slots the context
+// already holds if more (free memory no longer counts them), at most 64 and nk.
 static int choose_batch(const fame_ctx* c, int nk, const fame_solver_params* p, bool vec) {
   if (p->batch > 0) return std::min(p->batch, nk);
   size_t free_b = 0, total_b = 0;
   FAME_CK(cudaMemGetInfo(&free_b, &total_b));
   const bool mixed = p->precision == FAME_MIXED;
   const double per = slot_bytes(c, p->nstep, p->nwant, mixed, vec);
-  const int b = (int)std::max(1.0, floor(0.6 * (double)free_b / per));
+  const int b = std::max((int)std::max(1.0, floor(0.6 * (double)free_b / per)),
+                         held_slots(c, p->nstep, p->nwant, mixed, vec));
   return std::max(1, std::min({b, nk, 64}));
 }
 
@@ -1303,10 +1313,14 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
     // the G lanes (lane contexts allocate their workspace on their first solve)
     size_t free_b = 0, total_b = 0;
     FAME_CK(cudaMemGetInfo(&free_b, &total_b));
-    const double per = slot_bytes(c, prm->nstep, prm->nwant, prm->precision == FAME_MIXED,
-                                  prm->want_vectors || resabs_out);
+    const bool mixed = prm->precision == FAME_MIXED, vec = prm->want_vectors || resabs_out;
+    const double per = slot_bytes(c, prm->nstep, prm->nwant, mixed, vec);
     const int cap = (int)std::max(1.0, std::min(64.0, floor(0.6 * (double)free_b / (G * per))));
-    for (int i = 0; i < G; i++) pl[i].batch = std::min(cap, (int)((long)nk * (i + 1) / G - (long)nk * i / G));
+    for (int i = 0; i < G; i++) {
+      const fame_ctx* l = i == 0 ? c : c->lane_ctx[i - 1];
+      const int held = std::min(64, held_slots(l, prm->nstep, prm->nwant, mixed, vec));
+      pl[i].batch = std::min(std::max(cap, held), (int)((long)nk * (i + 1) / G - (long)nk * i / G));
+    }
   } catch (const CudaError& e) {
     set_err(e.what());
     return FAME_ERR_CUDA;
