@@ -148,6 +148,7 @@ WORKLOADS = {
     "bcc12": (_bcc_rods, 12, 2, bcc_eps(), 1.0, 12, 40),
     "bcc48": (_bcc_rods, 48, 2, bcc_eps(), 1.0, 12, 40),
     "hex12": (_hex_honeycomb, 12, 2, [11.4], 1.0, 16, 40),
+    "hex36": (_hex_honeycomb, 36, 2, [11.4], 1.0, 16, 40),
     "hex128": (_hex_honeycomb, 128, 2, [11.4], 1.0, 16, 40),
 }
 

@@ -1,6 +1,6 @@
 """Generates the golden fixtures in tests/golden/ from the reference's own build.
 
-    python tests/golden/make_golden.py pre            # CPU, needs the reference sources
+    python tests/golden/make_golden.py pre [NAME ...] # CPU, needs the reference sources
     python tests/golden/make_golden.py ref OUTDIR     # on a B200, runs the reference's
                                                       # FP64 CUDA solver (oracle/_ref)
     python tests/golden/make_golden.py condense OUTDIR
@@ -10,6 +10,7 @@
     python tests/golden/make_golden.py condense-path OUTDIR
     python tests/golden/make_golden.py ref-adjoint OUTDIR   # on a B200: adjoint config
     python tests/golden/make_golden.py condense-adjoint OUTDIR
+    python tests/golden/make_golden.py gamma-oracle         # CPU: hex36 Gamma spectrum
 
 `pre` runs the reference's preprocessing (FAME_Preprocessing) through
 oracle/_ref/fame_ref_harness for every named workload and stores its integer and
@@ -39,7 +40,7 @@ import ref_inputs as ri  # noqa: E402
 
 GOLDEN = os.path.dirname(os.path.abspath(__file__))
 
-PRE_NAMES = ["sc16", "sc32", "sc96", "fcc16", "fcc64", "bcc12", "bcc48", "hex12", "hex128"]
+PRE_NAMES = ["sc16", "sc32", "sc96", "fcc16", "fcc64", "bcc12", "bcc48", "hex12", "hex36", "hex128"]
 
 
 def material_dict(name):
@@ -58,8 +59,8 @@ def material_dict(name):
         lattice_type=m["lattice_type"], const=list(m["const"]))
 
 
-def do_pre():
-    for name in PRE_NAMES:
+def do_pre(names=None):
+    for name in names or PRE_NAMES:
         with tempfile.TemporaryDirectory() as d:
             ri.make_workdir(name, d)
             p = ri.run_pre(d, os.path.join(d, "pre.bin"))
@@ -248,6 +249,53 @@ def condense_adjoint(src, dst=GOLDEN):
                         es_iter=rec["es_iter"], ls_iter=rec["ls_iter"])
 
 
+def do_gamma_oracle(name="hex36", nwant=16, seed=7):
+    """Spectrum of A_r at the Gamma point of a hexagonal grid from an independent solver.
+
+    ARPACK (scipy eigsh, implicitly restarted Lanczos from a seeded random start) on
+    the oracle's A_r^-1, with the oracle's CG at a relative tolerance of 1e-13: the
+    nwant smallest eigenvalues of A_r on its N - 1 null-space-free columns, as
+    frequencies sqrt(lambda) with their relative residuals ||A_r v - lambda v|| /
+    (lambda ||v||).  Beside them, the oracle's restatement of the reference's solver
+    (Lanczos started at e_M, FAME_Fast_Algorithms_Isotropic.cu:20-86) on the same
+    k-point: whether that start reaches every band of this grid.  Writes
+    <name>_gamma_oracle.json; CPU only, about a minute."""
+    import scipy.sparse.linalg as sla
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import fame_oracle as fo
+    from fixtures import edge_eps, load_pre
+    par = load_pre(name)
+    B = edge_eps(par)
+    kidx = [int(i) for i in np.where(np.linalg.norm(par["kpoints"], axis=1) < 1e-3)[0]]
+    k = par["kpoints"][kidx[0]]
+    L = fo.lambdas(k, par)
+    assert L.Nd == par["N"] - 1
+    invB = 1.0 / B
+    s = np.concatenate([L.Lq_sqrt, L.Lq_sqrt])
+    M = 2 * L.Nd
+    ar = lambda x: s * fo.QBQ(s * x, L, invB)
+    op = sla.LinearOperator((M, M), dtype=complex,
+                            matvec=lambda x: fo.invAr(x, L, invB, 1e-13 * np.linalg.norm(x), 4000))
+    rng = np.random.default_rng(seed)
+    v0 = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    th, V = sla.eigsh(op, k=nwant, which="LA", v0=v0, ncv=3 * nwant, tol=1e-13)
+    order = np.argsort(1.0 / th)
+    lam = 1.0 / th[order]
+    res = [float(np.linalg.norm(ar(V[:, i]) - l * V[:, i]) / (l * np.linalg.norm(V[:, i])))
+           for i, l in zip(order, lam)]
+    ref_alg = fo.solve_k(k, par, B, dict(nwant=nwant, nstep=40, tol=1e-10, maxit=100),
+                         dict(tol=1e-10, maxit=1000))
+    out = dict(workload=name, grid=list(par["grid"]), gamma_kidx=kidx, Nd=int(L.Nd),
+               note="ARPACK (scipy eigsh, seeded random start) on the oracle's A_r^-1 at Gamma; "
+                    "freq = sqrt of the smallest eigenvalues of A_r, without the two zero bands",
+               freq=[float(v) for v in np.sqrt(lam)], relres=res,
+               from_e_M=dict(freq=[float(v) for v in ref_alg.freq], es_iter=int(ref_alg.es_iter),
+                             restarts=int(ref_alg.restarts), converged=bool(ref_alg.converged)))
+    with open(os.path.join(GOLDEN, f"{name}_gamma_oracle.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print(name, out["freq"], max(res))
+
+
 def condense(src, dst=GOLDEN):
     """Keeps the committed part of a `ref` run: all frequencies and counters, and
     the operator applications at k-points 0 (Gamma) and 1 only."""
@@ -274,7 +322,7 @@ def condense(src, dst=GOLDEN):
 
 if __name__ == "__main__":
     if sys.argv[1] == "pre":
-        do_pre()
+        do_pre(sys.argv[2:])
     elif sys.argv[1] == "ref":
         do_ref(sys.argv[2])
     elif sys.argv[1] == "condense":
@@ -291,5 +339,7 @@ if __name__ == "__main__":
         do_ref_adjoint(sys.argv[2])
     elif sys.argv[1] == "condense-adjoint":
         condense_adjoint(sys.argv[2])
+    elif sys.argv[1] == "gamma-oracle":
+        do_gamma_oracle()
     else:
         raise SystemExit(__doc__)

@@ -128,6 +128,30 @@ def test_gamma_point_patch():
     assert np.allclose(out["evec"][0, 0], v) and np.allclose(out["evec"][0, 1], v)
 
 
+@pytest.mark.parametrize("precision,tol", [(fb.FP64, 1e-8), (fb.MIXED, 1e-6)])
+def test_hexagonal_gamma_matches_an_independent_eigensolver(precision, tol):
+    """Hexagonal 36x30x26 (the hex 128 crystal on a grid an independent solver can
+    handle), at the path's two Gamma points: the two zero bands, then every band up to
+    the 14th of ARPACK's spectrum of A_r (tests/golden/hex36_gamma_oracle.json,
+    seeded random start on the oracle's A_r^-1), degenerate pairs included."""
+    import json
+    import os
+    par = load_pre("hex36")
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hex36_gamma_oracle.json")) as f:
+        orc = json.load(f)
+    ctx = _ctx(par)
+    k = par["kpoints"][orc["gamma_kidx"]]
+    out = ctx.solve(k, nwant=16, precision=precision, **TOL)
+    assert out["rc"] == fb.OK
+    ref = np.array(orc["freq"][:14])
+    for row, c in zip(out["freq"], out["counters"]):
+        assert c["Nd"] == par["N"] - 1
+        assert row[0] == 0 and row[1] == 0
+        assert np.max(np.abs(row[2:] - ref) / ref) < tol
+    assert np.all(out["relres"][:, 2:] < 1e-6)
+    ctx.close()
+
+
 def test_precision_and_batch_changes_on_one_context():
     """One context grows its batch in mixed precision (1 then 3 k-points) and then
     solves the same 3 k-points in FP64: every workspace buffer follows the largest

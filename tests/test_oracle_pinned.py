@@ -16,7 +16,7 @@ from fixtures import edge_eps, load_apply, load_pre, load_ref
 APPLY = ["sc16", "fcc16", "bcc12", "hex12"]
 
 
-@pytest.mark.parametrize("name", ["sc16", "sc32", "fcc16", "bcc12", "hex12", "bcc48", "fcc64"])
+@pytest.mark.parametrize("name", ["sc16", "sc32", "fcc16", "bcc12", "hex12", "hex36", "bcc48", "fcc64"])
 def test_binout_bit_exact(name):
     par = load_pre(name)
     b = fo.material_locate(par, par["material"])
@@ -99,3 +99,25 @@ def test_reference_band_path_fixtures(name, fix, per_seg, nk):
     gamma = np.linalg.norm(k, axis=1) < 1e-3
     assert np.all(nd[gamma] == par["N"] - 1) and np.all(nd[~gamma] == par["N"])
     assert np.all(np.diff(np.array([r["freq"] for r in ref["kpoints"]]), axis=1) >= 0)
+
+
+def test_hex36_gamma_fixture_agrees_with_the_reference_algorithm():
+    """The hex 36x30x26 Gamma fixture (make_golden.py gamma-oracle): ARPACK's eigenpairs
+    of A_r have relative residuals below 1e-10 and include the degenerate pairs; the
+    oracle's restatement of the reference's solver, started at e_M on the same k-point,
+    returns the two zero bands and then the same 14 frequencies to 1e-9.  (On the hex
+    128x107x92 grid the reference's own build returns only part of this spectrum at
+    Gamma; the GPU test compares this library's Gamma solve with the ARPACK list.)"""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hex36_gamma_oracle.json")) as f:
+        orc = json.load(f)
+    par = load_pre("hex36")
+    assert orc["Nd"] == par["N"] - 1
+    assert all(np.linalg.norm(par["kpoints"][i]) < 1e-3 for i in orc["gamma_kidx"])
+    f = np.array(orc["freq"])
+    assert np.all(np.diff(f) >= 0) and max(orc["relres"]) < 1e-10
+    assert np.sum(np.abs(np.diff(f)) < 1e-9 * f[1:]) >= 4  # degenerate pairs
+    e = orc["from_e_M"]
+    assert e["converged"] and e["freq"][:2] == [0.0, 0.0]
+    assert np.max(np.abs(np.array(e["freq"][2:]) - f[:14]) / f[:14]) < 1e-9
