@@ -1060,12 +1060,23 @@ int fame_set_material(fame_ctx* c, const int* binout, int material_num, const do
   return fame_set_eps(c, B.data());
 }
 
+// false when any of the n wave vectors has a NaN or infinite component
+static bool finite_k(const double* k, long n) {
+  for (long i = 0; i < 3 * n; i++)
+    if (!std::isfinite(k[i])) return false;
+  return true;
+}
+
 // One context's solve of nk k-points in batches (the body of fame_solve_kpoints).
 static int solve_batched(fame_ctx* c, const double* k_xyz, int nk, const fame_solver_params* prm,
                          double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
                          double* evec_out, fame_kcounters* counters) {
   if (!c || !k_xyz || !prm || !freq_out || nk <= 0) {
     set_err("null or empty argument");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (!finite_k(k_xyz, nk)) {
+    set_err("wave vector with a NaN or infinite component");
     return FAME_ERR_BAD_INPUT;
   }
   if (!c->have_eps) {
@@ -1298,7 +1309,7 @@ int fame_solve_kpoints(fame_ctx* c, const double* k_xyz, int nk, const fame_solv
                        double* freq_out, double* relres_out, double* relerr_out, double* resabs_out,
                        double* evec_out, fame_kcounters* counters) {
   int G = 1;
-  if (c && k_xyz && prm && freq_out && nk > 0 && c->have_eps && prm->batch == 0 &&
+  if (c && k_xyz && prm && freq_out && nk > 0 && finite_k(k_xyz, nk) && c->have_eps && prm->batch == 0 &&
       !(prm->want_vectors && !evec_out) && c->lanes > 1)
     G = std::min(c->lanes, nk / 4);
   if (G <= 1)
@@ -1367,6 +1378,10 @@ int fame_apply(fame_ctx* c, int op, const double* k, const void* in, void* out, 
   }
   if ((op == FAME_OP_QBQ || op == FAME_OP_INVAR) && !c->have_eps) {
     set_err("permittivity not set");
+    return FAME_ERR_BAD_INPUT;
+  }
+  if (!finite_k(k, 1)) {
+    set_err("wave vector with a NaN or infinite component");
     return FAME_ERR_BAD_INPUT;
   }
   try {

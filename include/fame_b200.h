@@ -125,6 +125,10 @@ int fame_set_material(fame_ctx* ctx, const int* binout, int material_num, const 
  *              want_vectors set and evec_out NULL the eigenvectors stay on the device
  *              for fame_adjoint_vjp (all nk k-points must fit one batch);
  *   counters   nk entries, or NULL.
+ * FAME_ERR_BAD_INPUT, before any device work: NULL k_xyz, params or freq_out, nk < 1,
+ * a wave vector with a NaN or infinite component, no permittivity set, parameters
+ * outside 1 <= nwant < nstep <= 64, es_maxit >= 0, ls_maxit >= 1, tolerances > 0, or
+ * a precision other than FAME_FP64 / FAME_MIXED.
  * Replaces FAME_Fast_Algorithms_Driver (FAME_Main/FAME_Main_Code.cu:142-171) over
  * the k-loop of FAME_Main_Code (:79-133). */
 int fame_solve_kpoints(fame_ctx* ctx, const double* k_xyz, int nk, const fame_solver_params* params,

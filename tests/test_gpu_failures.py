@@ -10,7 +10,9 @@ permittivities it divides by (FAME_Main/FAME_Matrix_B_Isotropic.cu:62-66).  Here
   - Lanczos without restarts (es_maxit = 0) at a tight tolerance sets
     FAME_KSTATUS_LANCZOS;
   - a loop bound set with fame_set_loop_cap that the CG loop reaches ends the solve
-    with FAME_ERR_WATCHDOG, and the context stays usable afterwards.
+    with FAME_ERR_WATCHDOG, and the context stays usable afterwards;
+  - solve arguments out of range (no k-points, a non-finite wave vector, band and
+    step counts, tolerances, precision, no permittivity yet) are FAME_ERR_BAD_INPUT.
 All inputs are host-side; no kernel is made to fault or hang."""
 import numpy as np
 import pytest
@@ -41,6 +43,50 @@ def test_bad_permittivity_is_rejected(bad):
     k = par["kpoints"][1:2]
     out = ctx.solve(k, nwant=4, nstep=20, es_tol=1e-8, ls_tol=1e-8)
     assert out["rc"] == fb.OK
+    ctx.close()
+
+
+BAD_SOLVES = [
+    ("no k-points", dict(k=np.zeros((0, 3)))),
+    ("NaN wave vector", dict(k=np.array([[0.1, np.nan, 0.2]]))),
+    ("infinite wave vector", dict(k=np.array([[np.inf, 0.0, 0.0]]))),
+    ("nwant = nstep", dict(nwant=20, nstep=20)),
+    ("nwant < 1", dict(nwant=0)),
+    ("nstep above 64", dict(nstep=65)),
+    ("zero Lanczos tolerance", dict(es_tol=0.0)),
+    ("NaN CG tolerance", dict(ls_tol=np.nan)),
+    ("ls_maxit < 1", dict(ls_maxit=0)),
+    ("negative es_maxit", dict(es_maxit=-1)),
+    ("unknown precision", dict(precision=7)),
+]
+
+
+@pytest.mark.parametrize("what,bad", BAD_SOLVES, ids=[b[0] for b in BAD_SOLVES])
+def test_invalid_solve_arguments_are_rejected(what, bad):
+    """Every argument fame_solve_kpoints rejects returns FAME_ERR_BAD_INPUT with a
+    message, and the context then solves normally.  The reference has no such checks:
+    its k-loop takes the Popt.txt values as they are (FAME_Main/FAME_Main_Code.cu:79-133)."""
+    par, ctx = _ctx()
+    bad = dict(bad)
+    k = bad.pop("k", par["kpoints"][1:2])
+    kw = dict(nwant=4, nstep=20, es_tol=1e-8, ls_tol=1e-8)
+    kw.update(bad)
+    with pytest.raises(fb.FameError) as e:
+        ctx.solve(k, **kw)
+    assert e.value.code == fb.ERR_BAD_INPUT, what
+    assert str(e.value).split(": ", 1)[1]  # the library's message
+    out = ctx.solve(par["kpoints"][1:2], nwant=4, nstep=20, es_tol=1e-8, ls_tol=1e-8)
+    assert out["rc"] == fb.OK
+    ctx.close()
+
+
+def test_solve_before_permittivity_is_rejected():
+    par = load_pre("sc16")
+    ctx = fb.Context.from_par(par)
+    with pytest.raises(fb.FameError) as e:
+        ctx.solve(par["kpoints"][1:2], nwant=4, nstep=20)
+    assert e.value.code == fb.ERR_BAD_INPUT
+    assert "permittivity" in str(e.value)
     ctx.close()
 
 
