@@ -456,6 +456,18 @@ template <> const float2* Ops::tw<float>() const { return c->tw32.p; }
 static int setup_geom(fame_ctx* c) {
   Geom& g = c->g;
   std::string err;
+  for (int i = 0; i < 3; i++)
+    if (!(c->lat.mesh_len[i] > 0.0) || !std::isfinite(c->lat.mesh_len[i])) {
+      set_err("mesh lengths must be finite and positive");
+      return FAME_ERR_BAD_INPUT;
+    }
+  bool finite = true;
+  for (double v : c->lat.lattice_vec_a) finite = finite && std::isfinite(v);
+  for (double v : c->lat.t1) finite = finite && std::isfinite(v);
+  if (!finite) {
+    set_err("lattice vectors and shifts must be finite");
+    return FAME_ERR_BAD_INPUT;
+  }
   const int rc = layout_geom(c->lat, g, 1L << 28, err);
   if (rc != FAME_OK) {
     set_err(err);

@@ -96,7 +96,11 @@ typedef struct {
 #define FAME_KSTATUS_CG 4      /* an A_r^-1 solve stopped above ls_tol: ls_maxit products (FP64) or
                                   the refinement cap (FAME_MIXED) */
 
-/* Create a context on `device` for one lattice/grid.  Allocates nothing per k yet. */
+/* Create a context on `device` for one lattice/grid.  Allocates nothing per k yet.
+ * FAME_ERR_BAD_INPUT before any allocation: a grid dimension below 2, a mesh length
+ * that is not finite and positive, a lattice vector or shift that is not finite.
+ * FAME_ERR_UNSUPPORTED: an axis needing more than 10 FFT passes, or an FP64 plane
+ * (mid x fast) beyond one CTA's shared memory. */
 int fame_ctx_create(int device, const fame_lattice* lat, fame_ctx** out);
 void fame_ctx_destroy(fame_ctx* ctx);
 

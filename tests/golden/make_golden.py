@@ -11,6 +11,7 @@
     python tests/golden/make_golden.py ref-adjoint OUTDIR   # on a B200: adjoint config
     python tests/golden/make_golden.py condense-adjoint OUTDIR
     python tests/golden/make_golden.py gamma-oracle         # CPU: hex36 Gamma spectrum
+    python tests/golden/make_golden.py hex36-oracle         # CPU: hex36 off-Gamma oracle solves
 
 `pre` runs the reference's preprocessing (FAME_Preprocessing) through
 oracle/_ref/fame_ref_harness for every named workload and stores its integer and
@@ -296,6 +297,32 @@ def do_gamma_oracle(name="hex36", nwant=16, seed=7):
     print(name, out["freq"], max(res))
 
 
+def do_hex36_oracle(name="hex36", kidx=(1, 2, 4), nwant=16):
+    """The oracle's FP64 solves (the restated reference algorithm: e_M start, CGS
+    Lanczos with lock/purge, CG at an absolute 1e-10) of three off-Gamma vertices of the
+    hex 36x30x26 path (M, K and A), with their Lanczos counts.  Writes
+    <name>_oracle.json; CPU only, about two minutes."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import fame_oracle as fo
+    from fixtures import edge_eps, load_pre
+    par = load_pre(name)
+    B = edge_eps(par)
+    recs = []
+    for q in kidx:
+        r = fo.solve_k(par["kpoints"][q], par, B, dict(nwant=nwant, nstep=40, tol=1e-10, maxit=100),
+                       dict(tol=1e-10, maxit=1000))
+        assert r.converged and r.Nd == par["N"]
+        recs.append(dict(kidx=int(q), wave_vec=[float(v) for v in par["kpoints"][q]],
+                         freq=[float(v) for v in r.freq], es_iter=int(r.es_iter), ls_iter=int(r.ls_iter),
+                         restarts=int(r.restarts)))
+        print(name, q, r.es_iter, r.freq[:4])
+    out = dict(workload=name, grid=list(par["grid"]), tol=1e-10, nwant=nwant,
+               note="oracle/fame_oracle.py solve_k (FP64 numpy restatement of the reference's solver)",
+               kpoints=recs)
+    with open(os.path.join(GOLDEN, f"{name}_oracle.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def condense(src, dst=GOLDEN):
     """Keeps the committed part of a `ref` run: all frequencies and counters, and
     the operator applications at k-points 0 (Gamma) and 1 only."""
@@ -341,5 +368,7 @@ if __name__ == "__main__":
         condense_adjoint(sys.argv[2])
     elif sys.argv[1] == "gamma-oracle":
         do_gamma_oracle()
+    elif sys.argv[1] == "hex36-oracle":
+        do_hex36_oracle()
     else:
         raise SystemExit(__doc__)

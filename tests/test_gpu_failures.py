@@ -80,6 +80,29 @@ def test_invalid_solve_arguments_are_rejected(what, bad):
     ctx.close()
 
 
+BAD_LATTICES = [
+    ("zero mesh length", dict(mesh_len=(0.0, 1 / 16, 1 / 16)), fb.ERR_BAD_INPUT),
+    ("NaN mesh length", dict(mesh_len=(1 / 16, np.nan, 1 / 16)), fb.ERR_BAD_INPUT),
+    ("infinite lattice vector", dict(lattice_vec_a=[np.inf] + [0.0] * 8), fb.ERR_BAD_INPUT),
+    ("grid below 2", dict(grid=(16, 1, 16)), fb.ERR_BAD_INPUT),
+    ("FP64 plane beyond one CTA", dict(grid=(200, 200, 4)), fb.ERR_UNSUPPORTED),
+]
+
+
+@pytest.mark.parametrize("what,bad,code", BAD_LATTICES, ids=[b[0] for b in BAD_LATTICES])
+def test_invalid_lattice_is_rejected(what, bad, code):
+    """fame_ctx_create checks the lattice before it allocates anything: grid dimensions
+    of at least 2, finite positive mesh lengths, finite lattice vectors, and a plane
+    that fits one CTA's shared memory."""
+    par = load_pre("sc16")
+    kw = dict(grid=par["grid"], mesh_len=par["mesh_len"], lattice_vec_a=par["lattice_vec_a"],
+              simple=par["simple"], m=par["m"], t1=par["t1"])
+    kw.update(bad)
+    with pytest.raises(fb.FameError) as e:
+        fb.Context(**kw)
+    assert e.value.code == code, what
+
+
 def test_solve_before_permittivity_is_rejected():
     par = load_pre("sc16")
     ctx = fb.Context.from_par(par)

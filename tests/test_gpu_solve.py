@@ -152,6 +152,27 @@ def test_hexagonal_gamma_matches_an_independent_eigensolver(precision, tol):
     ctx.close()
 
 
+def test_hexagonal_vertices_match_the_oracle():
+    """Hexagonal 36x30x26, the M, K and A vertices (tests/golden/hex36_oracle.json: the
+    oracle's FP64 restatement of the reference's solver at 1e-10): FP64 within 1e-8 and
+    mixed precision within 1e-6, with every band's relative residual below 1e-6.  The
+    grid's axes (36 = 4 x 9, 30 = 2 x 3 x 5, 26 = 2 x 13) run the runtime-geometry plans."""
+    import json
+    import os
+    par = load_pre("hex36")
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hex36_oracle.json")) as f:
+        orc = json.load(f)
+    k = np.array([r["wave_vec"] for r in orc["kpoints"]])
+    fr = np.array([r["freq"] for r in orc["kpoints"]])
+    ctx = _ctx(par)
+    for precision, tol in ((fb.FP64, 1e-8), (fb.MIXED, 1e-6)):
+        out = ctx.solve(k, nwant=orc["nwant"], precision=precision, **TOL)
+        assert out["rc"] == fb.OK
+        assert _relerr(out["freq"], fr) < tol, precision
+        assert np.all(out["relres"] < 1e-6)
+    ctx.close()
+
+
 def test_precision_and_batch_changes_on_one_context():
     """One context grows its batch in mixed precision (1 then 3 k-points) and then
     solves the same 3 k-points in FP64: every workspace buffer follows the largest
