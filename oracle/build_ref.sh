@@ -5,7 +5,7 @@
 #
 #   oracle/build_ref.sh REFERENCE_ROOT      (the reference project's root directory)
 #
-# Outputs (git-ignored, they travel to the GPU box with the tree):
+# Outputs (git-ignored):
 #   oracle/_ref/fame_ref_main     the reference's own Main.cpp program
 #   oracle/_ref/fame_ref_harness  oracle/ref_harness.cu linked with every reference
 #                                 object except Main.o

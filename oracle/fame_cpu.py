@@ -1,8 +1,8 @@
 """ctypes binding of oracle/fame_cpu.cpp (oracle/_build/libfame_cpu.so): the C++ /
 OpenMP FP64 restatement of the plain method on Simple lattices.
 
-TEST INFRASTRUCTURE ONLY: tests/ and the cpu_baseline leg of bench.py use it as a
-checker and as the CPU baseline.  The product never imports it."""
+TEST INFRASTRUCTURE ONLY: tests/ and the cpu_baseline leg of bench.py use it to
+check results and as the CPU baseline.  The product never imports it."""
 from __future__ import annotations
 
 import ctypes as C

@@ -1,7 +1,7 @@
 """CPU FP64 restatement of FAME-Isotropic-GPU's band-structure path (numpy).
 
 TEST INFRASTRUCTURE ONLY.  This module is the oracle: tests/, the smoke check and
-the cpu_baseline leg of bench.py may import it as a checker.  The product (the
+the cpu_baseline leg of bench.py may import it, to check results.  The product (the
 CUDA library behind include/fame_b200.h) never imports, links or calls it.
 
 Every function follows one reference routine and cites it (paths are relative
