@@ -61,7 +61,8 @@ def test_qrs_qr_identity():
     assert np.linalg.norm(fo.Qrs(fo.Qr(x, L), L) - x) <= 1e-12 * np.linalg.norm(x)
 
 
-@pytest.mark.parametrize("name,kidx", [("sc16", 1), ("sc16", 0), ("bcc12", 2)])
+@pytest.mark.parametrize("name,kidx", [("sc16", 1), ("sc16", 0), ("bcc12", 2), ("hex12", 0), ("hex12", 1),
+                                       ("fcc16", 1)])
 def test_solve_matches_reference_frequencies(name, kidx):
     par = load_pre(name)
     ref = load_ref(name)
