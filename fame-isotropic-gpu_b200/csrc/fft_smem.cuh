@@ -427,11 +427,13 @@ __device__ __forceinline__ void generic_pass(cplx<R>* buf, int n, int r, int Ns,
 // FMAs per 2*ML + MU shared-memory loads.  cos/sin come from the axis table,
 // tw[(us mod r)*nb] = e^{-2 pi i us/r}.  Returns false (nothing done) when one
 // line's MU-groups exceed the block; the caller then takes the output-stationary
-// pass.
-template <typename R, int MU, int ML>
+// pass.  TC > 0: the block's thread count as a compile-time constant (static plans,
+// whose kernels launch exactly TC threads), so that the cell and line split, the
+// rounds and the shared-memory offsets fold to constants; 0: blockDim.x.
+template <typename R, int MU, int ML, int TC = 0>
 __device__ __forceinline__ bool prime_pass(cplx<R>* buf, int n, int r, int Ns, LineSet L, const cplx<R>* tw,
                                            bool inv) {
-  const int T = blockDim.x;
+  const int T = TC > 0 ? TC : (int)blockDim.x;
   const int nb = n / r;
   const int stw = n / (Ns * r);
   const int H = (r - 1) / 2;
@@ -711,7 +713,7 @@ __device__ __forceinline__ void sfft(cplx<R>* buf, int ls, int es, const cplx<R>
     if constexpr (RAD >= 17) {
       // a prime factor >= 17: the symmetric-pair pass, its sizes compile-time constants
       const LineSet L{NL, ls, es};
-      if (!prime_pass<R, PrimeBlock<R>::mu, PrimeBlock<R>::ml>(buf, N, RAD, NS, L, tw, inv))
+      if (!prime_pass<R, PrimeBlock<R>::mu, PrimeBlock<R>::ml, T>(buf, N, RAD, NS, L, tw, inv))
         generic_pass<R, EMAX>(buf, N, RAD, NS, L, tw, inv);
     } else {
       constexpr int MB = smaxb(N, NL, T, EMAX, RAD);
