@@ -520,8 +520,9 @@ def run_lattices(args):
     hexagonal 128x107x92; the reference's preprocessing outputs in tests/golden/)
     at the tolerance of the reference's runs on the same B200 (1e-10): the non-Gamma
     vertices of each path, mixed precision and FP64, timed with CUDA events on the
-    context's stream after one warm-up solve.  The reference's k-points/s are its own
-    measured per-k wall times from those runs (tests/golden/<name>_ref.json)."""
+    context's stream after a warm-up solve of the same k-points.  The reference's
+    k-points/s are its own measured per-k wall times from those runs
+    (tests/golden/<name>_ref.json)."""
     import torch
     import fame_b200 as fb
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -548,7 +549,7 @@ def run_lattices(args):
         for prec, tag in ((fb.MIXED, "mixed"), (fb.FP64, "fp64")):
             p = fb.solver_params(nwant=nw, nstep=NSTEP, es_tol=ref["tol"], ls_tol=ref["tol"], es_maxit=100,
                                  ls_maxit=1000, precision=prec)
-            ctx.solve(k[:1], p)
+            ctx.solve(k, p)  # warm-up on the same k-points: lane contexts and graphs exist before timing
             st = torch.cuda.ExternalStream(ctx.stream())
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()

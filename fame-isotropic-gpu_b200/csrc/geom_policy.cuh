@@ -53,6 +53,13 @@ template <> struct SEmax<double> { static constexpr int v = 12; };
 template <typename R> struct SPenEmax;
 template <> struct SPenEmax<float> { static constexpr int v = 24; };
 template <> struct SPenEmax<double> { static constexpr int v = 12; };
+// static plane passes of the runtime-geometry grids (128 registers at two 256-thread
+// CTAs per SM, the general-lattice Pi mixing in the same kernel): half the 96^3
+// staging, which keeps the radix-11 and radix-13 passes of the FCC and BCC planes
+// in registers (FCC 64x55x52: FP32 CG iteration 37.5 -> 33.9 us per k-point)
+template <typename R> struct PlaneEmax;
+template <> struct PlaneEmax<float> { static constexpr int v = 12; };
+template <> struct PlaneEmax<double> { static constexpr int v = 6; };
 
 // DynGeom with the slow-axis length fixed at compile time: the pencil stage's
 // slow-axis transforms run the static plan (unrolled passes, constant strides and
@@ -82,9 +89,9 @@ struct DynGeomPlane : DynGeom {
   __device__ __forceinline__ static void fft_plane(cplx<R>* b, const Geom&, bool fast, const cplx<R>* tw,
                                                    bool inv) {
     if (fast)
-      sfft<R, LF, LM, T, SEmax<R>::v>(b, LF | 1, 1, tw, inv);
+      sfft<R, LF, LM, T, PlaneEmax<R>::v>(b, LF | 1, 1, tw, inv);
     else
-      sfft<R, LM, LF, T, SEmax<R>::v>(b, 1, LF | 1, tw, inv);
+      sfft<R, LM, LF, T, PlaneEmax<R>::v>(b, 1, LF | 1, tw, inv);
   }
 };
 
