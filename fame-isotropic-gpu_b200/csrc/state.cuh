@@ -5,9 +5,12 @@
 
 namespace fame {
 
-// complex elements a thread holds in registers during one FFT pass (per precision)
+// complex elements a thread holds in registers during one FFT pass of the runtime
+// plans (per precision).  FP32 stages 8: the runtime plane kernels run at 64
+// registers, and 16 elements spilled twice as much (FP32 CG iteration on the
+// runtime plans of FCC 64x55x52: 38.6 -> 36.3 us per k-point, hex 36x30x26: 14.8 -> 13.6)
 template <typename R> struct Emax;
-template <> struct Emax<float> { static constexpr int v = 16; };
+template <> struct Emax<float> { static constexpr int v = 8; };
 template <> struct Emax<double> { static constexpr int v = 8; };
 // fast-axis positions per pencil CTA: 256-byte rows
 template <typename R> struct PencilTW { static constexpr int v = 256 / (int)sizeof(cplx<R>); };
