@@ -55,11 +55,12 @@ template <> struct SPenEmax<float> { static constexpr int v = 24; };
 template <> struct SPenEmax<double> { static constexpr int v = 12; };
 // static plane passes of the runtime-geometry grids (128 registers at two 256-thread
 // CTAs per SM, the general-lattice Pi mixing in the same kernel): half the 96^3
-// staging, which keeps the radix-11 and radix-13 passes of the FCC and BCC planes
-// in registers (FCC 64x55x52: FP32 CG iteration 37.5 -> 33.9 us per k-point)
+// staging in FP32, a third in FP64, which keeps the radix-11 and radix-13 passes of
+// the FCC and BCC planes in registers (FCC 64x55x52: FP32 CG iteration 37.5 -> 33.9
+// us per k-point; BCC 48x45x39: FP64 plane stages 23.5 -> 20.7 us)
 template <typename R> struct PlaneEmax;
 template <> struct PlaneEmax<float> { static constexpr int v = 12; };
-template <> struct PlaneEmax<double> { static constexpr int v = 6; };
+template <> struct PlaneEmax<double> { static constexpr int v = 4; };
 // static slow-axis passes of the runtime-geometry grids (80 registers at three
 // pencil CTAs per SM, the general-lattice twiddles in the same kernel): a third of
 // the 96^3 pencil staging, which removes the FP32 spills (hexagonal 128-point slow
